@@ -1,0 +1,213 @@
+/*
+ * wtivo_gpupr.h -- C ABI of the B200 graph-cut library (libwtivo_gpupr.so).
+ *
+ * The min s-t cut over the Delaunay tet cell graph of WTiVo: reduced-graph
+ * build, multi-discharge push-relabel with exact global relabels, and the
+ * final residual BFS that fixes the source/sink partition.  Plain pointers
+ * and sizes only; no exceptions cross this boundary; every entry point
+ * returns a gpupr_status and keeps a human-readable detail message that
+ * gpupr_last_error() returns (per thread).
+ *
+ * Streams: `stream` is a cudaStream_t passed as void* (NULL = the legacy
+ * default stream).  Calls return after their results are complete.
+ */
+#ifndef WTIVO_GPUPR_H
+#define WTIVO_GPUPR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPUPR_ABI_VERSION 1
+
+typedef enum {
+    GPUPR_OK = 0,
+    GPUPR_ERR_INVALID_ARGUMENT = 1,  /* shapes/pointers (bindings.cpp:114-133) */
+    GPUPR_ERR_NEIGHBOR_RANGE = 2,    /* "neighbor out of range" (bindings.cpp:172) */
+    GPUPR_ERR_REFS_ODD = 3,          /* "neighbor reference count not even" (:177) */
+    GPUPR_ERR_BUILD = 4,             /* "invalid graph reduction/capacity state" (:297) */
+    GPUPR_ERR_FREE_REFS_ODD = 5,     /* "free reference count not even" (:318) */
+    GPUPR_ERR_TOO_MANY_NODES = 6,    /* ">INT32_MAX reduced nodes unsupported" (:198) */
+    GPUPR_ERR_NO_REVERSE = 7,        /* asymmetric adjacency (.cu:129,254 codes 2/4) */
+    GPUPR_ERR_OUT_OF_MEMORY = 8,     /* "insufficient VRAM ..." (:212) */
+    GPUPR_ERR_MAX_ROUNDS = 9,        /* "max macro rounds exceeded" (.cu:492) */
+    GPUPR_ERR_INVARIANT = 10,        /* device invariant failed (.cu:206,292) */
+    GPUPR_ERR_CUDA = 11,             /* CUDA runtime failure (.cu:23-29) */
+    GPUPR_ERR_TIMEOUT = 12,          /* solve time limit (.cu:542-543) / bounded wait */
+    GPUPR_ERR_TOO_MANY_TETS = 13     /* ">2^32 full tets unsupported" (:132) */
+} gpupr_status;
+
+/* Statistics of one graph_cut call.  The first 18 fields are the 18-tuple of
+ * graph_cut_fast (bindings.cpp:377-396) in order. */
+typedef struct {
+    int64_t adjusted_flow;      /* raw_flow + terminal base flow */
+    int64_t raw_flow;           /* flow pushed into the sink by the solver */
+    uint64_t graph_bytes;       /* device bytes of the reduced graph */
+    uint64_t workspace_bytes;   /* device bytes of the solver workspace */
+    uint64_t full_E;            /* faces between finite tets */
+    uint64_t free_E;            /* faces between free tets */
+    uint64_t fixed_source;
+    uint64_t fixed_sink;
+    uint64_t terminal_edges;
+    int64_t threads;            /* echoed max(1, threads) */
+    uint64_t rounds;            /* discharge rounds */
+    uint64_t global_relabels;   /* exact BFS relabels, the final one included */
+    uint64_t map_bytes;         /* N*4 + F*4 */
+    double build_seconds;       /* classify + reduced-graph build */
+    int64_t local_steps;        /* echoed as passed */
+    double solve_seconds;       /* push-relabel until the active set is empty */
+    double native_total_seconds;
+    /* extensions */
+    uint64_t free_n;
+    uint64_t n_full;
+    double final_relabel_seconds;
+    double partition_seconds;
+    uint64_t node_visits;       /* discharge node visits */
+    uint64_t pushes;            /* arc pushes (sink pushes included) */
+    uint64_t bfs_visits;        /* frontier nodes expanded by BFS levels */
+    uint64_t bfs_levels;        /* BFS levels over all global relabels */
+    uint64_t kernel_launches;   /* kernels this call launched */
+    double solve_device_ms;     /* CUDA-event time of the solve phase */
+    double build_device_ms;     /* CUDA-event time of the build phase */
+    double discharge_ms;        /* CUDA-event time of all discharge batches */
+    double bfs_ms;              /* CUDA-event time of all global-relabel BFS */
+    uint64_t discharge_launches;
+    uint64_t bfs_launches;
+} gpupr_cut_stats;
+
+/* Solver tuning knobs; zero fields take the defaults shown. */
+typedef struct {
+    int32_t local_steps;          /* 1..32, default 8 */
+    int32_t global_relabel_period;/* old-equivalent rounds (default 1024) */
+    uint64_t max_rounds;          /* default 2,000,000 */
+    double time_limit_seconds;    /* default 240 */
+    int32_t round_batch;          /* rounds enqueued per host check, default 24 */
+    int32_t bfs_batch;            /* BFS levels enqueued per host check, default 48 */
+    int32_t block_size;           /* threads per block, default 256 */
+    int32_t blocks_per_sm;        /* persistent grid multiplier, default 4 */
+    double work_relabel_factor;   /* relabel after this many node visits per
+                                     free node since the last one (default 3) */
+} gpupr_solve_options;
+
+const char* gpupr_status_string(gpupr_status status);
+const char* gpupr_last_error(void);
+int gpupr_abi_version(void);
+
+/*
+ * Whole graph_cut_fast path.
+ * Replaces graph_cut_gpupr_fast_v630 (native/gpupr/wtivo_gpupr_bindings.cpp:
+ * 100-397) behind wtivo_gpupr.graph_cut_fast (:581-590).
+ *   vertices   float64 [n_vertices*3]   host (vertices_on_device=0) or device
+ *   d_tets     int32   [n_tets*4]        device
+ *   d_neighbors int32  [n_tets*4]        device, CelloCut slots, -1 = hull
+ *   labels     uint8   [n_tets]          host or device
+ *   out_labels uint8   [n_tets]          host or device: input labels with
+ *              every free tet replaced by 1 iff it reaches the sink
+ * threads is only echoed in the stats (the build runs on the GPU).
+ * local_steps, global_relabel_period and max_rounds keep the reference's
+ * meaning and clamps (gpu_push_relabel_fast.cu:421-424,476-480).
+ * When no tet is free the output equals the input labels and
+ * stats->free_n == 0 (bindings.cpp:191-196).
+ */
+gpupr_status gpupr_graph_cut(const double* vertices, uint64_t n_vertices,
+                             int vertices_on_device, const int32_t* d_tets,
+                             const int32_t* d_neighbors, uint64_t n_tets,
+                             const uint8_t* labels, int labels_on_device,
+                             double fill_T, int32_t threads,
+                             int32_t global_relabel_period, uint64_t max_rounds,
+                             int32_t local_steps, uint8_t* out_labels,
+                             int out_on_device, void* stream,
+                             gpupr_cut_stats* stats);
+
+/* Same as gpupr_graph_cut with explicit solver options (NULL = defaults). */
+gpupr_status gpupr_graph_cut_ex(const double* vertices, uint64_t n_vertices,
+                                int vertices_on_device, const int32_t* d_tets,
+                                const int32_t* d_neighbors, uint64_t n_tets,
+                                const uint8_t* labels, int labels_on_device,
+                                double fill_T, int32_t threads,
+                                const gpupr_solve_options* options,
+                                uint8_t* out_labels, int out_on_device,
+                                void* stream, gpupr_cut_stats* stats);
+
+/*
+ * Reduced-graph build only (bindings.cpp:146-314): writes the reference's
+ * host arrays so the build can be compared byte for byte.  All outputs are
+ * HOST buffers sized by the caller: full_to_free[n_tets], free_old[n_tets],
+ * nbr[4*n_tets], res[4*n_tets], term[n_tets], rev[n_tets] (2-bit reverse
+ * slots, slot k in bits 2k..2k+1).  info[8] = {free_n, fixed_source,
+ * fixed_sink, full_refs, free_refs, terminal_edges, terminal_base_flow,
+ * n_tets}.
+ */
+gpupr_status gpupr_build_reduced(const double* vertices, uint64_t n_vertices,
+                                 int vertices_on_device, const int32_t* d_tets,
+                                 const int32_t* d_neighbors, uint64_t n_tets,
+                                 const uint8_t* labels, int labels_on_device,
+                                 double fill_T, int32_t* full_to_free,
+                                 uint32_t* free_old, int32_t* nbr, uint32_t* res,
+                                 int32_t* term, uint8_t* rev, int64_t* info,
+                                 void* stream);
+
+/*
+ * Phase-I solve of a reduced graph already in device memory.
+ * Replaces cellocut_gpu_push_relabel_fast
+ * (native/gpupr/gpu_push_relabel_fast.h:20-28, .cu:406-571): same layout
+ * (d_neighbors int32[4n], d_residual uint32[4n], d_terminal int32[n], both
+ * updated in place to the final residual graph), h_partition uint8[n] on the
+ * host (1 = reaches the sink).  d_excess_out (optional, device int64[n])
+ * receives the final preflow excess.
+ */
+gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors,
+                                 uint32_t* d_residual, int32_t* d_terminal,
+                                 uint8_t* h_partition,
+                                 int32_t global_relabel_period,
+                                 uint64_t max_rounds, int32_t local_steps,
+                                 int64_t* d_excess_out, void* stream,
+                                 gpupr_cut_stats* stats);
+
+/*
+ * Raw-graph entry (no reduction): every node is free, n-links cap[4n] in
+ * CelloCut ELL slots (nbr -1 = none), source capacities src[n] and sink
+ * capacities snk[n].  All inputs are DEVICE buffers and are not modified.
+ * Outputs: *max_flow (host) and d_partition uint8[n] (device, 1 = reaches
+ * the sink; the minimal sink side of the minimum cut).  No reference
+ * counterpart: it serves integer-capacity graphs that do not come from
+ * graph_cut_fast's reduction.
+ */
+gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr,
+                             const uint32_t* d_cap, const uint32_t* d_src,
+                             const uint32_t* d_snk,
+                             const gpupr_solve_options* options,
+                             int64_t* max_flow, uint8_t* d_partition,
+                             void* stream, gpupr_cut_stats* stats);
+
+/*
+ * Cut-surface extraction.  Replaces surface_extraction_topology_cuda
+ * (bindings.cpp:400-577): the oriented boundary faces of label-0 tets in the
+ * reference's order, with vertices compacted in original order.  Two-step:
+ * gpupr_surface_count() returns the face and used-vertex counts and keeps the
+ * result on the device for the next gpupr_surface_fetch() on the same
+ * thread.  labels and vertices are host or device; tets/neighbors device.
+ */
+gpupr_status gpupr_surface_count(const uint8_t* labels, int labels_on_device,
+                                 const double* vertices, uint64_t n_vertices,
+                                 int vertices_on_device, const int32_t* d_tets,
+                                 const int32_t* d_neighbors, uint64_t n_tets,
+                                 uint64_t* n_faces, uint64_t* n_used,
+                                 void* stream);
+gpupr_status gpupr_surface_fetch(int32_t* faces, double* vertices_out,
+                                 int out_on_device, void* stream);
+
+/* Release device memory cached between calls (pool + scratch). */
+gpupr_status gpupr_release_cached_memory(void);
+
+/* Bounded-wait self test: a device loop waits on a flag that nothing sets,
+ * gives up after about `limit_us` microseconds and returns
+ * GPUPR_ERR_TIMEOUT with the context still usable. */
+gpupr_status gpupr_selftest_bounded_wait(uint32_t limit_us, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

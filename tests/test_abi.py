@@ -1,0 +1,95 @@
+"""C-ABI library and drop-in module on the CPU: they load, export every
+declared symbol, and reject bad arguments with the reference's messages
+before touching a GPU (native/gpupr/wtivo_gpupr_bindings.cpp:114-133)."""
+from __future__ import annotations
+
+import ctypes
+import inspect
+
+import numpy as np
+import pytest
+import torch
+
+
+def test_library_exports_header(built):
+    import gpupr_capi
+
+    names = gpupr_capi.header_functions()
+    assert "gpupr_graph_cut" in names and "gpupr_solve_reduced" in names
+    L = ctypes.CDLL(str(gpupr_capi.LIB_PATH))
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert gpupr_capi.lib().gpupr_abi_version() == 1
+    assert gpupr_capi.lib().gpupr_status_string(9) == b"GPUPr-FAST-v6.30 max macro rounds exceeded"
+
+
+def test_module_exports_reference_names(built):
+    import wtivo_gpupr
+
+    for name in ("graph_cut_fast", "graph_cut_gpupr_fast_v630", "surface_extraction_topology_cuda"):
+        assert hasattr(wtivo_gpupr, name)
+    # keyword names are accepted (validation fails later, on the vertices)
+    t = torch.zeros((2, 4), dtype=torch.int32)
+    kw = dict(tets_cuda=t, neighbors_cuda=t, labels=np.ones(2, np.uint8), fill_T=10.0, threads=16,
+              global_relabel_period=1024, max_rounds=2000000, local_steps=8)
+    for fn in (wtivo_gpupr.graph_cut_fast, wtivo_gpupr.graph_cut_gpupr_fast_v630):
+        with pytest.raises(RuntimeError, match="vertices must be float64 Nx3"):
+            fn(vertices=np.zeros((2, 2)), **kw)
+    with pytest.raises(RuntimeError, match="vertices must be float64 Nx3"):
+        wtivo_gpupr.surface_extraction_topology_cuda(labels=np.ones(2, np.uint8),
+                                                     vertices=np.zeros(3), tets_cuda=t,
+                                                     neighbors_cuda=t, threads=16)
+    doc = wtivo_gpupr.graph_cut_fast.__doc__.split("\n")[0]
+    pos = [doc.index(x) for x in ("threads:", "= 16", "global_relabel_period:", "= 1024",
+                                  "max_rounds:", "= 2000000", "local_steps:", "= 8")]
+    assert pos == sorted(pos)
+    assert "= 16" in wtivo_gpupr.surface_extraction_topology_cuda.__doc__
+
+
+def _args(n=8):
+    V = np.zeros((4, 3))
+    t = torch.zeros((n, 4), dtype=torch.int32)
+    lab = np.ones(n, np.uint8)
+    return V, t, t.clone(), lab
+
+
+def test_module_validation_order(built):
+    import wtivo_gpupr as g
+
+    V, t, nb, lab = _args()
+    with pytest.raises(RuntimeError, match="vertices must be float64 Nx3"):
+        g.graph_cut_fast(np.zeros((4, 2)), t, nb, lab, 10.0)
+    with pytest.raises(RuntimeError, match="tets/neighbors must be CUDA tensors"):
+        g.graph_cut_fast(V, t, nb, lab, 10.0)
+    with pytest.raises(RuntimeError, match="tets/neighbors must be contiguous CUDA int32 Nx4 with same N"):
+        g.surface_extraction_topology_cuda(lab, V, t, nb)
+    with pytest.raises(TypeError):
+        g.graph_cut_fast(V, "not a tensor", nb, lab, 10.0)
+
+
+def test_capi_rejects_host_topology(built):
+    """Host pointers for tets/neighbors are refused, not read."""
+    import gpupr_capi
+
+    st = gpupr_capi.CutStats()
+    tets = np.zeros((8, 4), np.int32)
+    lab = np.ones(8, np.uint8)
+    out = np.empty(8, np.uint8)
+    V = np.zeros((4, 3))
+    rc = gpupr_capi.lib().gpupr_graph_cut(
+        V.ctypes.data_as(ctypes.c_void_p), 4, 0, tets.ctypes.data_as(ctypes.c_void_p),
+        tets.ctypes.data_as(ctypes.c_void_p), 8, lab.ctypes.data_as(ctypes.c_void_p), 0, 10.0,
+        16, 1024, 0, 8, out.ctypes.data_as(ctypes.c_void_p), 0, None, ctypes.byref(st))
+    assert rc != 0
+    # an empty graph is a no-op that echoes threads/local_steps
+    rc = gpupr_capi.lib().gpupr_graph_cut(None, 0, 0, None, None, 0, None, 0, 10.0, 0, 1024, 0, 5,
+                                          None, 0, None, ctypes.byref(st))
+    assert rc == 0 and st.threads == 1 and st.local_steps == 5
+
+
+def test_python_side_is_plumbing_only():
+    """The drop-in path has no CPU solver to fall back to."""
+    import gpupr_capi
+
+    src = inspect.getsource(gpupr_capi)
+    assert "oracle" not in src.replace("no CPU fallback", "")

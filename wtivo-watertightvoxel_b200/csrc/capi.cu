@@ -1,0 +1,514 @@
+// capi.cu -- the C ABI of libwtivo_gpupr.so (include/wtivo_gpupr.h).
+//
+// Host orchestration of the graph_cut_fast path: argument checks with the
+// reference's messages (native/gpupr/wtivo_gpupr_bindings.cpp:114-133),
+// H2D of host-side vertices/labels, GPU reduced-graph build, solve, label
+// scatter (bindings.cpp:357-364), D2H of the result and the stats tuple.
+// No exception crosses the ABI: every entry point returns a gpupr_status
+// and records the message for gpupr_last_error().
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "gpupr_internal.cuh"
+#include "wtivo_gpupr.h"
+
+namespace gpupr {
+
+namespace {
+thread_local std::string g_last_error;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+
+cudaMemPool_t device_pool()
+{
+    int dev = 0;
+    GPUPR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "device ordinal out of range"};
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        GPUPR_CUDA(cudaMemPoolCreate(&g_pools[dev], &props));
+        // keep freed blocks for the next call: repeated cuts reuse the same
+        // footprint without cudaMalloc/cudaFree (gpupr_release_cached_memory
+        // trims the pool).
+        uint64_t keep = UINT64_MAX;
+        GPUPR_CUDA(cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    return g_pools[dev];
+}
+
+void select_device_for(const void* dptr, const char* what)
+{
+    cudaPointerAttributes a{};
+    cudaError_t e = cudaPointerGetAttributes(&a, dptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, std::string(what) + " must be CUDA tensors"};
+    }
+    if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, std::string(what) + " must be CUDA tensors"};
+    GPUPR_CUDA(cudaSetDevice(a.device));
+}
+
+bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+template <class Fn>
+gpupr_status guarded(Fn&& fn)
+{
+    try {
+        fn();
+        g_last_error.clear();
+        return GPUPR_OK;
+    } catch (const Error& e) {
+        g_last_error = e.msg;
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return GPUPR_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return GPUPR_ERR_CUDA;
+    } catch (...) {
+        g_last_error = "unknown failure";
+        return GPUPR_ERR_CUDA;
+    }
+}
+
+double seconds_since(std::chrono::steady_clock::time_point t0)
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+struct Timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaStream_t s;
+    explicit Timer(cudaStream_t st) : s(st)
+    {
+        GPUPR_CUDA(cudaEventCreate(&a));
+        GPUPR_CUDA(cudaEventCreate(&b));
+        GPUPR_CUDA(cudaEventRecord(a, s));
+    }
+    double stop_ms()
+    {
+        GPUPR_CUDA(cudaEventRecord(b, s));
+        GPUPR_CUDA(cudaEventSynchronize(b));
+        float ms = 0.f;
+        GPUPR_CUDA(cudaEventElapsedTime(&ms, a, b));
+        return ms;
+    }
+    ~Timer()
+    {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+// Device copies of host inputs (no copy when already on the device).
+template <class T>
+const T* on_device(const T* p, size_t count, int is_device, DevBuf<T>& keep, cudaStream_t s)
+{
+    if (is_device || count == 0) return p;
+    keep = DevBuf<T>(count, s);
+    GPUPR_CUDA(cudaMemcpyAsync(keep.p, p, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    return keep.p;
+}
+
+void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t* d_tets,
+                   const int32_t* d_nbrs, uint64_t N, const uint8_t* labels, int l_dev,
+                   double fill_T, int32_t threads, int32_t period, uint64_t max_rounds,
+                   int32_t local_steps, const gpupr_solve_options* options, uint8_t* out,
+                   int out_dev, cudaStream_t s, gpupr_cut_stats* st)
+{
+    const auto all0 = std::chrono::steady_clock::now();
+    if (!st) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "stats pointer is NULL"};
+    std::memset(st, 0, sizeof(*st));
+    st->threads = threads < 1 ? 1 : threads;
+    st->local_steps = local_steps;
+    st->n_full = N;
+    if (N > 0xFFFFFFFFull) throw Error{GPUPR_ERR_TOO_MANY_TETS, ">2^32 full tets unsupported"};
+    if (N == 0) {
+        st->native_total_seconds = seconds_since(all0);
+        return;
+    }
+    if (!d_tets || !d_nbrs) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets/neighbors must be CUDA tensors"};
+    if (!labels || !out) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "labels size mismatch"};
+    if (!vertices && nv) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "vertices must be float64 Nx3"};
+    if (!aligned(d_tets, 16) || !aligned(d_nbrs, 16))
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets/neighbors must be 16-byte aligned"};
+    select_device_for(d_tets, "tets/neighbors");
+
+    uint64_t launches = 0;
+    const auto b0 = std::chrono::steady_clock::now();
+    Timer tb(s);
+    DevBuf<uint8_t> dlab;
+    DevBuf<double> dver;
+    const uint8_t* d_labels = on_device(labels, N, l_dev, dlab, s);
+    const double* d_vertices = on_device(vertices, nv * 3u, v_dev, dver, s);
+    if (v_dev && vertices && !aligned(vertices, 8))
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "vertices must be float64 Nx3"};
+
+    BuildInputs in{d_vertices, nv, d_tets, d_nbrs, d_labels, N, fill_T};
+    ReducedGraph g;
+    BuildInfo info;
+    build_reduced_graph(in, g, info, s, &launches);
+    st->build_device_ms = tb.stop_ms();
+    st->build_seconds = seconds_since(b0);
+    st->full_E = info.full_refs / 2u;
+    st->fixed_source = info.fixed_source;
+    st->fixed_sink = info.fixed_sink;
+    st->free_n = info.free_n;
+
+    if (info.free_n == 0) {   // bindings.cpp:191-196: labels unchanged
+        if (out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, d_labels, N, cudaMemcpyDeviceToDevice, s));
+        else GPUPR_CUDA(cudaMemcpyAsync(out, d_labels, N, cudaMemcpyDeviceToHost, s));
+        GPUPR_CUDA(cudaStreamSynchronize(s));
+        st->kernel_launches = launches;
+        st->native_total_seconds = seconds_since(all0);
+        return;
+    }
+
+    const SolveOptions opt = resolve_options(options, local_steps, period, max_rounds);
+    SolveWorkspace w;
+    SolveResult sr;
+    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.term.p, w, opt, s, sr);
+    launches += sr.launches;
+
+    const auto p0 = std::chrono::steady_clock::now();
+    DevBuf<uint8_t> dout;
+    uint8_t* d_out = out;
+    if (!out_dev) {
+        dout = DevBuf<uint8_t>(N, s);
+        d_out = dout.p;
+    }
+    GPUPR_CUDA(cudaMemcpyAsync(d_out, d_labels, N, cudaMemcpyDeviceToDevice, s));
+    scatter_partition(g.n, g.free_old.p, w.height.p, d_out, s, &launches);
+    if (!out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, d_out, N, cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    st->partition_seconds = seconds_since(p0);
+
+    st->raw_flow = sr.raw_flow;
+    st->adjusted_flow = sr.raw_flow + info.terminal_base_flow;
+    st->graph_bytes = g.graph_bytes();
+    st->workspace_bytes = sr.workspace_bytes;
+    st->free_E = info.free_refs / 2u;
+    st->terminal_edges = info.terminal_edges;
+    st->rounds = sr.rounds;
+    st->global_relabels = sr.relabels;
+    st->map_bytes = N * 4u + (uint64_t)g.n * 4u;
+    st->solve_seconds = sr.solve_s;
+    st->final_relabel_seconds = sr.final_relabel_s;
+    st->node_visits = sr.node_visits;
+    st->pushes = sr.pushes;
+    st->bfs_visits = sr.bfs_visits;
+    st->bfs_levels = sr.bfs_levels;
+    st->solve_device_ms = sr.solve_device_ms;
+    st->discharge_ms = sr.discharge_ms;
+    st->bfs_ms = sr.bfs_ms;
+    st->discharge_launches = sr.discharge_launches;
+    st->bfs_launches = sr.bfs_launches;
+    st->kernel_launches = launches;
+    st->native_total_seconds = seconds_since(all0);
+}
+
+}  // namespace
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+void* pool_alloc(size_t bytes, cudaStream_t s)
+{
+    void* p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, device_pool(), s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{GPUPR_ERR_OUT_OF_MEMORY, "insufficient VRAM for reduced graph + solver (" +
+                                                 std::to_string(bytes) + " bytes: " +
+                                                 cudaGetErrorString(e) + ")"};
+    }
+    return p;
+}
+
+void pool_free(void* p, cudaStream_t s)
+{
+    if (p) cudaFreeAsync(p, s);
+}
+
+}  // namespace gpupr
+
+using namespace gpupr;
+
+extern "C" {
+
+const char* gpupr_status_string(gpupr_status status)
+{
+    switch (status) {
+    case GPUPR_OK: return "ok";
+    case GPUPR_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case GPUPR_ERR_NEIGHBOR_RANGE: return "neighbor out of range";
+    case GPUPR_ERR_REFS_ODD: return "neighbor reference count not even";
+    case GPUPR_ERR_BUILD: return "invalid graph reduction/capacity state";
+    case GPUPR_ERR_FREE_REFS_ODD: return "free reference count not even";
+    case GPUPR_ERR_TOO_MANY_NODES: return ">INT32_MAX reduced nodes unsupported";
+    case GPUPR_ERR_NO_REVERSE: return "device invariant failed (asymmetric adjacency)";
+    case GPUPR_ERR_OUT_OF_MEMORY: return "insufficient VRAM for reduced graph + solver";
+    case GPUPR_ERR_MAX_ROUNDS: return "GPUPr-FAST-v6.30 max macro rounds exceeded";
+    case GPUPR_ERR_INVARIANT: return "device invariant failed";
+    case GPUPR_ERR_CUDA: return "CUDA failure";
+    case GPUPR_ERR_TIMEOUT: return "time limit exceeded";
+    case GPUPR_ERR_TOO_MANY_TETS: return ">2^32 full tets unsupported";
+    }
+    return "unknown status";
+}
+
+const char* gpupr_last_error(void) { return g_last_error.c_str(); }
+
+int gpupr_abi_version(void) { return GPUPR_ABI_VERSION; }
+
+gpupr_status gpupr_graph_cut(const double* vertices, uint64_t n_vertices, int vertices_on_device,
+                             const int32_t* d_tets, const int32_t* d_neighbors, uint64_t n_tets,
+                             const uint8_t* labels, int labels_on_device, double fill_T,
+                             int32_t threads, int32_t global_relabel_period, uint64_t max_rounds,
+                             int32_t local_steps, uint8_t* out_labels, int out_on_device,
+                             void* stream, gpupr_cut_stats* stats)
+{
+    return guarded([&] {
+        run_graph_cut(vertices, n_vertices, vertices_on_device, d_tets, d_neighbors, n_tets, labels,
+                      labels_on_device, fill_T, threads, global_relabel_period, max_rounds,
+                      local_steps, nullptr, out_labels, out_on_device,
+                      static_cast<cudaStream_t>(stream), stats);
+    });
+}
+
+gpupr_status gpupr_graph_cut_ex(const double* vertices, uint64_t n_vertices, int vertices_on_device,
+                                const int32_t* d_tets, const int32_t* d_neighbors, uint64_t n_tets,
+                                const uint8_t* labels, int labels_on_device, double fill_T,
+                                int32_t threads, const gpupr_solve_options* options,
+                                uint8_t* out_labels, int out_on_device, void* stream,
+                                gpupr_cut_stats* stats)
+{
+    return guarded([&] {
+        const int32_t ls = options && options->local_steps ? options->local_steps : 8;
+        const int32_t per = options && options->global_relabel_period ? options->global_relabel_period : 1024;
+        const uint64_t mr = options && options->max_rounds ? options->max_rounds : 2000000ull;
+        run_graph_cut(vertices, n_vertices, vertices_on_device, d_tets, d_neighbors, n_tets, labels,
+                      labels_on_device, fill_T, threads, per, mr, ls, options, out_labels,
+                      out_on_device, static_cast<cudaStream_t>(stream), stats);
+    });
+}
+
+gpupr_status gpupr_build_reduced(const double* vertices, uint64_t n_vertices, int vertices_on_device,
+                                 const int32_t* d_tets, const int32_t* d_neighbors, uint64_t n_tets,
+                                 const uint8_t* labels, int labels_on_device, double fill_T,
+                                 int32_t* full_to_free, uint32_t* free_old, int32_t* nbr,
+                                 uint32_t* res, int32_t* term, uint8_t* rev, int64_t* info_out,
+                                 void* stream)
+{
+    return guarded([&] {
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (!info_out) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "info pointer is NULL"};
+        std::memset(info_out, 0, 8 * sizeof(int64_t));
+        info_out[7] = (int64_t)n_tets;
+        if (n_tets == 0) return;
+        if (n_tets > 0xFFFFFFFFull) throw Error{GPUPR_ERR_TOO_MANY_TETS, ">2^32 full tets unsupported"};
+        if (!d_tets || !d_neighbors || !labels || (!vertices && n_vertices))
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL input"};
+        if (!aligned(d_tets, 16) || !aligned(d_neighbors, 16))
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets/neighbors must be 16-byte aligned"};
+        select_device_for(d_tets, "tets/neighbors");
+        DevBuf<uint8_t> dlab;
+        DevBuf<double> dver;
+        const uint8_t* d_labels = on_device(labels, n_tets, labels_on_device, dlab, s);
+        const double* d_vertices = on_device(vertices, n_vertices * 3u, vertices_on_device, dver, s);
+        BuildInputs in{d_vertices, n_vertices, d_tets, d_neighbors, d_labels, n_tets, fill_T};
+        ReducedGraph g;
+        BuildInfo info;
+        uint64_t launches = 0;
+        build_reduced_graph(in, g, info, s, &launches);
+        info_out[0] = (int64_t)info.free_n;
+        info_out[1] = (int64_t)info.fixed_source;
+        info_out[2] = (int64_t)info.fixed_sink;
+        info_out[3] = (int64_t)info.full_refs;
+        info_out[4] = (int64_t)info.free_refs;
+        info_out[5] = (int64_t)info.terminal_edges;
+        info_out[6] = info.terminal_base_flow;
+        const size_t F = info.free_n;
+        if (full_to_free)
+            GPUPR_CUDA(cudaMemcpyAsync(full_to_free, g.full_to_free.p, n_tets * 4u, cudaMemcpyDeviceToHost, s));
+        if (F) {
+            if (free_old) GPUPR_CUDA(cudaMemcpyAsync(free_old, g.free_old.p, F * 4u, cudaMemcpyDeviceToHost, s));
+            if (nbr) GPUPR_CUDA(cudaMemcpyAsync(nbr, g.nbr.p, F * 16u, cudaMemcpyDeviceToHost, s));
+            if (res) GPUPR_CUDA(cudaMemcpyAsync(res, g.res.p, F * 16u, cudaMemcpyDeviceToHost, s));
+            if (term) GPUPR_CUDA(cudaMemcpyAsync(term, g.term.p, F * 4u, cudaMemcpyDeviceToHost, s));
+            if (rev) GPUPR_CUDA(cudaMemcpyAsync(rev, g.rev.p, F, cudaMemcpyDeviceToHost, s));
+        }
+        GPUPR_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_residual,
+                                 int32_t* d_terminal, uint8_t* h_partition,
+                                 int32_t global_relabel_period, uint64_t max_rounds,
+                                 int32_t local_steps, int64_t* d_excess_out, void* stream,
+                                 gpupr_cut_stats* stats)
+{
+    return guarded([&] {
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        if (!n) return;
+        if (!d_neighbors || !d_residual || !d_terminal || !h_partition)
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "GPUPr-FAST-v6.30 null graph pointer"};
+        if (!aligned(d_neighbors, 16) || !aligned(d_residual, 16))
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "graph rows must be 16-byte aligned"};
+        if (n > 0x7FFFFFFFu) throw Error{GPUPR_ERR_TOO_MANY_NODES, ">INT32_MAX reduced nodes unsupported"};
+        select_device_for(d_neighbors, "graph");
+        uint64_t launches = 0;
+        DevBuf<uint8_t> rev(n, s);
+        compute_reverse_slots(n, reinterpret_cast<const int4*>(d_neighbors), rev.p, s, &launches);
+        const SolveOptions opt = resolve_options(nullptr, local_steps, global_relabel_period, max_rounds);
+        SolveWorkspace w;
+        SolveResult sr;
+        solve_push_relabel(n, reinterpret_cast<const int4*>(d_neighbors), d_residual, rev.p,
+                           d_terminal, w, opt, s, sr);
+        launches += sr.launches;
+        DevBuf<uint8_t> part(n, s);
+        partition_from_height(n, w.height.p, part.p, s, &launches);
+        GPUPR_CUDA(cudaMemcpyAsync(h_partition, part.p, n, cudaMemcpyDeviceToHost, s));
+        if (d_excess_out)
+            GPUPR_CUDA(cudaMemcpyAsync(d_excess_out, w.excess.p, (size_t)n * 8u, cudaMemcpyDeviceToDevice, s));
+        GPUPR_CUDA(cudaStreamSynchronize(s));
+        if (stats) {
+            stats->raw_flow = sr.raw_flow;
+            stats->adjusted_flow = sr.raw_flow;
+            stats->workspace_bytes = sr.workspace_bytes;
+            stats->rounds = sr.rounds;
+            stats->global_relabels = sr.relabels;
+            stats->local_steps = local_steps;
+            stats->solve_seconds = sr.solve_s;
+            stats->final_relabel_seconds = sr.final_relabel_s;
+            stats->free_n = n;
+            stats->node_visits = sr.node_visits;
+            stats->pushes = sr.pushes;
+            stats->bfs_visits = sr.bfs_visits;
+            stats->bfs_levels = sr.bfs_levels;
+            stats->solve_device_ms = sr.solve_device_ms;
+            stats->discharge_ms = sr.discharge_ms;
+            stats->bfs_ms = sr.bfs_ms;
+            stats->discharge_launches = sr.discharge_launches;
+            stats->bfs_launches = sr.bfs_launches;
+            stats->kernel_launches = launches;
+        }
+    });
+}
+
+gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d_cap,
+                             const uint32_t* d_src, const uint32_t* d_snk,
+                             const gpupr_solve_options* options, int64_t* max_flow,
+                             uint8_t* d_partition, void* stream, gpupr_cut_stats* stats)
+{
+    return guarded([&] {
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        if (max_flow) *max_flow = 0;
+        if (!n) return;
+        if (!d_nbr || !d_cap || !d_src || !d_snk || !max_flow || !d_partition)
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL graph pointer"};
+        if (!aligned(d_nbr, 16) || !aligned(d_cap, 16))
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "graph rows must be 16-byte aligned"};
+        if (n > 0x7FFFFFFFu) throw Error{GPUPR_ERR_TOO_MANY_NODES, ">INT32_MAX nodes unsupported"};
+        select_device_for(d_nbr, "graph");
+        uint64_t launches = 0;
+        DevBuf<uint32_t> res((size_t)n * 4u, s);
+        DevBuf<int32_t> term(n, s);
+        DevBuf<uint8_t> rev(n, s);
+        const int64_t base = prepare_raw_graph(n, d_cap, d_src, d_snk, d_nbr, res.p, term.p, s, &launches);
+        compute_reverse_slots(n, reinterpret_cast<const int4*>(d_nbr), rev.p, s, &launches);
+        const SolveOptions opt = resolve_options(options, 8, 1024, 2000000ull);
+        SolveWorkspace w;
+        SolveResult sr;
+        solve_push_relabel(n, reinterpret_cast<const int4*>(d_nbr), res.p, rev.p, term.p, w, opt, s, sr);
+        launches += sr.launches;
+        partition_from_height(n, w.height.p, d_partition, s, &launches);
+        GPUPR_CUDA(cudaStreamSynchronize(s));
+        *max_flow = base + sr.raw_flow;
+        if (stats) {
+            stats->adjusted_flow = base + sr.raw_flow;
+            stats->raw_flow = sr.raw_flow;
+            stats->graph_bytes = res.bytes() + term.bytes() + rev.bytes();
+            stats->workspace_bytes = sr.workspace_bytes;
+            stats->rounds = sr.rounds;
+            stats->global_relabels = sr.relabels;
+            stats->local_steps = opt.local_steps;
+            stats->solve_seconds = sr.solve_s;
+            stats->final_relabel_seconds = sr.final_relabel_s;
+            stats->free_n = n;
+            stats->node_visits = sr.node_visits;
+            stats->pushes = sr.pushes;
+            stats->bfs_visits = sr.bfs_visits;
+            stats->bfs_levels = sr.bfs_levels;
+            stats->solve_device_ms = sr.solve_device_ms;
+            stats->discharge_ms = sr.discharge_ms;
+            stats->bfs_ms = sr.bfs_ms;
+            stats->discharge_launches = sr.discharge_launches;
+            stats->bfs_launches = sr.bfs_launches;
+            stats->kernel_launches = launches;
+        }
+    });
+}
+
+gpupr_status gpupr_surface_count(const uint8_t* labels, int labels_on_device, const double* vertices,
+                                 uint64_t n_vertices, int vertices_on_device, const int32_t* d_tets,
+                                 const int32_t* d_neighbors, uint64_t n_tets, uint64_t* n_faces,
+                                 uint64_t* n_used, void* stream)
+{
+    return guarded([&] {
+        if (!n_faces || !n_used) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL count pointer"};
+        *n_faces = 0;
+        *n_used = 0;
+        if (n_tets && (!d_tets || !d_neighbors || !labels))
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets/neighbors must be contiguous CUDA int32 Nx4 with same N"};
+        if (n_tets) {
+            if (!aligned(d_tets, 16) || !aligned(d_neighbors, 16))
+                throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets/neighbors must be 16-byte aligned"};
+            select_device_for(d_tets, "tets/neighbors");
+        }
+        surface_count(labels, labels_on_device, vertices, n_vertices, vertices_on_device, d_tets,
+                      d_neighbors, n_tets, n_faces, n_used, static_cast<cudaStream_t>(stream));
+    });
+}
+
+gpupr_status gpupr_surface_fetch(int32_t* faces, double* vertices_out, int out_on_device, void* stream)
+{
+    return guarded([&] { surface_fetch(faces, vertices_out, out_on_device, static_cast<cudaStream_t>(stream)); });
+}
+
+gpupr_status gpupr_release_cached_memory(void)
+{
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        for (int d = 0; d < 64; ++d)
+            if (g_pools[d]) GPUPR_CUDA(cudaMemPoolTrimTo(g_pools[d], 0));
+    });
+}
+
+gpupr_status gpupr_selftest_bounded_wait(uint32_t limit_us, void* stream)
+{
+    gpupr_status result = GPUPR_OK;
+    gpupr_status st = guarded([&] {
+        result = bounded_wait_selftest(limit_us, static_cast<cudaStream_t>(stream));
+        if (result == GPUPR_ERR_TIMEOUT) g_last_error = "bounded wait gave up after the limit";
+    });
+    if (st != GPUPR_OK) return st;
+    if (result == GPUPR_ERR_TIMEOUT) g_last_error = "bounded wait gave up after the limit";
+    return result;
+}
+
+}  // extern "C"

@@ -1,0 +1,219 @@
+// gpupr_internal.cuh -- shared device structures and helpers of the B200
+// graph-cut library.  Not part of the public ABI (include/wtivo_gpupr.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "wtivo_gpupr.h"
+
+namespace gpupr {
+
+// Unreached / unlabelled height.  Any height >= n (the free-node count) is
+// inactive, exactly like the reference's source_h = n, inf_h = n + 1
+// (gpu_push_relabel_fast.cu:426-427); UNVIS also marks "not visited" during
+// a BFS, so no normalisation pass is needed (.cu:141-147 becomes a no-op).
+constexpr uint32_t UNVIS = 0xFFFFFFFFu;
+
+// Device control block: ring counters for the double-buffered queues, flags
+// and work counters.  One per solve; zeroed at solve start.
+struct Ctl {
+    uint32_t act_cnt[3];     // active queue sizes, ring indexed by round % 3
+    uint32_t bfs_cnt[3];     // BFS frontier sizes, ring indexed by level % 3
+    uint32_t bfs_done;       // a level found an empty frontier
+    uint32_t bfs_levels;     // levels expanded (non-empty) in this BFS
+    int32_t error;           // first device invariant failure (status code)
+    uint32_t error_node;
+    uint32_t rounds_done;    // non-empty discharge rounds this phase
+    uint32_t level_base;     // current BFS level (graph-launched batches)
+    unsigned long long sink_flow;
+    unsigned long long node_visits;
+    unsigned long long pushes;
+    unsigned long long bfs_visits;
+    unsigned long long relabels;
+    unsigned long long reserved[4];
+};
+
+// View of the reduced graph + solver workspace handed to kernels.
+struct SolveView {
+    uint32_t n;
+    const int4* __restrict__ nbr;       // [n] neighbor row (reduced ids, -1)
+    uint32_t* res;                      // [4n] residual capacity per slot
+    const uint8_t* __restrict__ rev;    // [n] 2-bit reverse slot per slot
+    int32_t* term;                      // [n] src - snk residual
+    long long* excess;                  // [n]
+    uint32_t* height;                   // [n]
+    uint32_t* act[2];                   // active queues (double buffered)
+    uint32_t* fr[2];                    // BFS frontiers (fr[1] aliases act[1])
+    Ctl* ctl;
+    int local_steps;
+};
+
+// ---------------------------------------------------------------------------
+// Host-side helpers
+// ---------------------------------------------------------------------------
+struct Error {
+    gpupr_status status;
+    std::string msg;
+};
+
+void set_last_error(const std::string& msg);
+
+#define GPUPR_CUDA(expr)                                                     \
+    do {                                                                     \
+        cudaError_t _e = (expr);                                             \
+        if (_e != cudaSuccess)                                               \
+            throw ::gpupr::Error{_e == cudaErrorMemoryAllocation             \
+                                     ? GPUPR_ERR_OUT_OF_MEMORY               \
+                                     : GPUPR_ERR_CUDA,                       \
+                                 std::string("GPUPr-B200 CUDA failure at ") + \
+                                     #expr + ": " + cudaGetErrorString(_e)}; \
+    } while (0)
+
+// Stream-ordered device allocation from the library's pool.
+void* pool_alloc(size_t bytes, cudaStream_t s);
+void pool_free(void* p, cudaStream_t s);
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    DevBuf() = default;
+    DevBuf(size_t count, cudaStream_t st) : n(count), s(st)
+    {
+        if (count) p = static_cast<T*>(pool_alloc(count * sizeof(T), st));
+    }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept
+    {
+        if (this != &o) { reset(); p = o.p; n = o.n; s = o.s; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevBuf() { reset(); }
+    void reset()
+    {
+        if (p) pool_free(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// Launch geometry: number of SMs of the current device (cached).
+int sm_count();
+
+// ---------------------------------------------------------------------------
+// Reduced-graph build (graph_build.cu)
+// ---------------------------------------------------------------------------
+struct BuildInputs {
+    const double* d_vertices;   // device [nv*3]
+    uint64_t nv;
+    const int32_t* d_tets;      // device [N*4]
+    const int32_t* d_nbrs;      // device [N*4]
+    const uint8_t* d_labels;    // device [N]
+    uint64_t N;
+    double fill_T;
+};
+
+struct BuildInfo {
+    uint64_t free_n = 0, fixed_source = 0, fixed_sink = 0, full_refs = 0;
+    uint64_t free_refs = 0, terminal_edges = 0;
+    int64_t terminal_base_flow = 0;
+};
+
+struct ReducedGraph {
+    uint32_t n = 0;
+    DevBuf<int4> nbr;
+    DevBuf<uint32_t> res;       // 4n
+    DevBuf<uint8_t> rev;
+    DevBuf<int32_t> term;
+    DevBuf<int32_t> full_to_free;  // N
+    DevBuf<uint32_t> free_old;     // n
+    uint64_t graph_bytes() const { return nbr.bytes() + res.bytes() + rev.bytes() + term.bytes(); }
+};
+
+// Classify + compact + build; throws gpupr::Error with reference messages.
+void build_reduced_graph(const BuildInputs& in, ReducedGraph& g, BuildInfo& info,
+                         cudaStream_t s, uint64_t* launches);
+
+// Exclusive scan of per-tile counts (one block); *d_total receives the sum.
+void scan_tile_counts(uint32_t ntiles, const uint32_t* d_cnt, unsigned long long* d_off,
+                      unsigned long long* d_total, cudaStream_t s, uint64_t* launches);
+
+// Reverse-slot table for a reduced graph given in the reference layout.
+void compute_reverse_slots(uint32_t n, const int4* d_nbr, uint8_t* d_rev, cudaStream_t s,
+                           uint64_t* launches);
+
+// label scatter: out[free_old[q]] = height[q] != UNVIS
+void scatter_partition(uint32_t n, const uint32_t* d_free_old, const uint32_t* d_height,
+                       uint8_t* d_out, cudaStream_t s, uint64_t* launches);
+void partition_from_height(uint32_t n, const uint32_t* d_height, uint8_t* d_part,
+                           cudaStream_t s, uint64_t* launches);
+
+// ---------------------------------------------------------------------------
+// Solver (push_relabel.cu)
+// ---------------------------------------------------------------------------
+struct SolveOptions {
+    int local_steps = 8;
+    int relabel_rounds = 128;      // ceil(period / local_steps), 0 = only when idle
+    uint64_t max_rounds = 2000000ull;
+    double time_limit_s = 240.0;
+    int round_batch = 24;
+    int bfs_batch = 48;
+    int block = 256;
+    int blocks_per_sm = 4;
+    double work_factor = 3.0;
+};
+
+SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw,
+                             int period_raw, uint64_t max_rounds_raw);
+
+struct SolveWorkspace {
+    DevBuf<long long> excess;
+    DevBuf<uint32_t> height;
+    DevBuf<uint32_t> q0, q1, q2;
+    DevBuf<Ctl> ctl;
+    uint64_t bytes() const
+    {
+        return excess.bytes() + height.bytes() + q0.bytes() + q1.bytes() + q2.bytes() + ctl.bytes();
+    }
+};
+
+struct SolveResult {
+    int64_t raw_flow = 0;
+    uint64_t rounds = 0, relabels = 0, node_visits = 0, pushes = 0, bfs_visits = 0,
+             bfs_levels = 0, launches = 0;
+    double solve_s = 0.0, final_relabel_s = 0.0, solve_device_ms = 0.0;
+    double discharge_ms = 0.0, bfs_ms = 0.0;
+    uint64_t discharge_launches = 0, bfs_launches = 0;
+    uint64_t workspace_bytes = 0;
+};
+
+// Phase-I push-relabel on a reduced graph (res/term updated in place).
+// On return the workspace heights mark the sink-reachable set
+// (height != UNVIS) of the final residual graph.
+void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const uint8_t* d_rev,
+                        int32_t* d_term, SolveWorkspace& w, const SolveOptions& opt,
+                        cudaStream_t s, SolveResult& out);
+
+// Cut-surface extraction (surface.cu): count keeps its result per thread
+// for the following fetch.
+void surface_count(const uint8_t* labels, int l_dev, const double* vertices, uint64_t nv, int v_dev,
+                   const int32_t* d_tets, const int32_t* d_nbrs, uint64_t N, uint64_t* n_faces,
+                   uint64_t* n_used, cudaStream_t s);
+void surface_fetch(int32_t* faces, double* verts, int out_dev, cudaStream_t s);
+
+// Bounded wait self test kernel driver.
+gpupr_status bounded_wait_selftest(uint32_t limit_us, cudaStream_t s);
+
+// Raw ELL graph: res = cap, term = src - snk, returns base flow sum min(src,snk).
+int64_t prepare_raw_graph(uint32_t n, const uint32_t* d_cap, const uint32_t* d_src,
+                          const uint32_t* d_snk, const int32_t* d_nbr, uint32_t* d_res,
+                          int32_t* d_term, cudaStream_t s, uint64_t* launches);
+
+}  // namespace gpupr

@@ -1,0 +1,571 @@
+// push_relabel.cu -- Phase-I multi-discharge push-relabel on the reduced
+// ELL graph, with exact global relabels by backward BFS from the sink.
+//
+// Replaces cellocut_gpu_push_relabel_fast
+// (native/gpupr/gpu_push_relabel_fast.cu:406-571).  Differences in design:
+//
+//  * No host round trip per round or per BFS level: kernels read their
+//    queue sizes from a device control block (ring counters), and the host
+//    enqueues batches of rounds/levels and checks the state once per batch.
+//  * Reverse slots are precomputed at build time (2 bits per slot), so a push
+//    or a BFS step never searches the neighbor's row (.cu:56-67).
+//  * Queue de-duplication without flags: a node owns its excess; the thread
+//    whose atomic add moves a node's excess from 0 to positive enqueues it,
+//    and a discharged node that keeps excess re-enqueues itself (.cu:168-178
+//    used a queued[] flag and a CAS per enqueue).
+//  * Queue appends are staged in shared memory and written with one global
+//    atomic per block iteration; sink flow and work counters are reduced per
+//    block.
+//  * Exactness by construction: the solve ends only when an exact global
+//    relabel finds no node with excess that can reach the sink, so the
+//    returned preflow is maximum and the sink-reachable set is the minimal
+//    sink side of the minimum cut (the reference stops when its queue
+//    empties, .cu:490, then relabels once, .cu:551-556).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <chrono>
+#include <cmath>
+#include <string>
+
+#include "gpupr_internal.cuh"
+
+namespace gpupr {
+namespace {
+
+constexpr int DTPB = 256;   // block size of the solver kernels
+
+__device__ __forceinline__ uint32_t ldcg(const uint32_t* p) { return __ldcg(p); }
+__device__ __forceinline__ int32_t ldcg(const int32_t* p) { return __ldcg(p); }
+__device__ __forceinline__ long long ldcg(const long long* p) { return __ldcg(p); }
+
+template <class T>
+__device__ __forceinline__ T warp_block_sum(T v, T* sh)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    T t = 0;
+    if (threadIdx.x < 32) {
+        t = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : T(0);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    }
+    return t;
+}
+
+__global__ void __launch_bounds__(DTPB) k_init_excess(uint32_t n, const int32_t* __restrict__ term,
+                                                      long long* __restrict__ excess)
+{
+    for (uint32_t v = blockIdx.x * DTPB + threadIdx.x; v < n; v += gridDim.x * DTPB) {
+        const int32_t t = term[v];
+        excess[v] = t > 0 ? (long long)t : 0ll;   // source arc saturated (.cu:69-83)
+    }
+}
+
+// Level 1 of the backward BFS: nodes with a residual arc to the sink.  Every
+// other height is reset to UNVIS (.cu:374-379).
+__global__ void __launch_bounds__(DTPB) k_bfs_seed(SolveView g)
+{
+    __shared__ uint32_t s_fr[DTPB], s_act[DTPB];
+    __shared__ uint32_t s_fc, s_ac, s_fn, s_an, s_fb, s_ab;
+    Ctl* ctl = g.ctl;
+    if (threadIdx.x == 0) { s_fc = 0; s_ac = 0; }
+    __syncthreads();
+    for (uint32_t base = blockIdx.x * DTPB; base < g.n; base += gridDim.x * DTPB) {
+        const uint32_t v = base + threadIdx.x;
+        if (v < g.n) {
+            const int32_t t = ldcg(g.term + v);
+            g.height[v] = (t < 0) ? 1u : UNVIS;
+            if (t < 0) {
+                s_fr[atomicAdd(&s_fc, 1u)] = v;
+                if (1u < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_ac, 1u)] = v;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_fn = s_fc; s_an = s_ac; s_fc = 0; s_ac = 0;
+            s_fb = s_fn ? atomicAdd(&ctl->bfs_cnt[1], s_fn) : 0u;
+            s_ab = s_an ? atomicAdd(&ctl->act_cnt[0], s_an) : 0u;
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < s_fn; j += DTPB) g.fr[1][s_fb + j] = s_fr[j];
+        for (uint32_t j = threadIdx.x; j < s_an; j += DTPB) g.act[0][s_ab + j] = s_act[j];
+        __syncthreads();
+    }
+}
+
+// One top-down BFS level L: frontier nodes u (height L) label every
+// unvisited neighbor v with a residual arc v->u as L+1 (.cu:103-139).
+__global__ void __launch_bounds__(DTPB) k_bfs_level(SolveView g, uint32_t L)
+{
+    __shared__ uint32_t s_fr[DTPB * 4], s_act[DTPB * 4];
+    __shared__ uint32_t s_fc, s_ac, s_fn, s_an, s_fb, s_ab;
+    __shared__ unsigned long long s_red[DTPB / 32];
+    Ctl* ctl = g.ctl;
+    const uint32_t cnt = ldcg(&ctl->bfs_cnt[L % 3]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->bfs_cnt[(L + 2) % 3] = 0u;
+        if (cnt == 0) ctl->bfs_done = 1u;
+        else atomicAdd(&ctl->bfs_levels, 1u);
+    }
+    if (cnt == 0) return;
+    const uint32_t* in = (L & 1) ? g.fr[1] : g.fr[0];
+    uint32_t* out = (L & 1) ? g.fr[0] : g.fr[1];
+    uint32_t* gcnt = &ctl->bfs_cnt[(L + 1) % 3];
+    const uint32_t newh = L + 1u;
+    unsigned long long visits = 0;
+    if (threadIdx.x == 0) { s_fc = 0; s_ac = 0; }
+    __syncthreads();
+    for (uint32_t base = blockIdx.x * DTPB; base < cnt; base += gridDim.x * DTPB) {
+        const uint32_t i = base + threadIdx.x;
+        if (i < cnt) {
+            const uint32_t u = __ldg(in + i);
+            const int4 nb4 = __ldg(g.nbr + u);
+            const uint32_t rv = __ldg(g.rev + u);
+            const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+            ++visits;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int v = nb[k];
+                if (v < 0) continue;
+                if (ldcg(g.height + v) != UNVIS) continue;
+                const uint32_t rk = (rv >> (2 * k)) & 3u;
+                if (ldcg(g.res + (size_t)v * 4u + rk) == 0u) continue;
+                if (atomicCAS(g.height + v, UNVIS, newh) == UNVIS) {
+                    s_fr[atomicAdd(&s_fc, 1u)] = (uint32_t)v;
+                    if (newh < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_ac, 1u)] = (uint32_t)v;
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_fn = s_fc; s_an = s_ac; s_fc = 0; s_ac = 0;
+            s_fb = s_fn ? atomicAdd(gcnt, s_fn) : 0u;
+            s_ab = s_an ? atomicAdd(&ctl->act_cnt[0], s_an) : 0u;
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < s_fn; j += DTPB) out[s_fb + j] = s_fr[j];
+        for (uint32_t j = threadIdx.x; j < s_an; j += DTPB) g.act[0][s_ab + j] = s_act[j];
+        __syncthreads();
+    }
+    const unsigned long long vs = warp_block_sum(visits, s_red);
+    if (threadIdx.x == 0 && vs) atomicAdd(&ctl->bfs_visits, vs);
+}
+
+struct Work {
+    unsigned long long visits = 0, pushes = 0, relabels = 0, sink = 0;
+};
+
+// Discharge one active node for up to local_steps push/relabel steps
+// (.cu:185-313).  Pushes go to residual arcs whose neighbor is lower,
+// lowest first; the sink (height 0) is used when h == 1.  The relabel
+// lifts v to 1 + the lowest residual neighbor.  Neighbor heights are read
+// once per visit; stale values only cost work, never exactness (see the
+// file comment).
+__device__ __forceinline__ void discharge_node(const SolveView& g, uint32_t v, uint32_t* s_buf,
+                                               uint32_t* s_cnt, Work& w)
+{
+    const uint32_t n = g.n;
+    uint32_t h = g.height[v];
+    if (h >= n) return;
+    long long ex = ldcg(g.excess + v);
+    if (ex <= 0) return;
+    const int4 nb4 = __ldg(g.nbr + v);
+    const uint4 r4 = __ldcg(reinterpret_cast<const uint4*>(g.res) + v);
+    const uint32_t rv = __ldg(g.rev + v);
+    int32_t t = g.term[v];
+    const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+    uint32_t r[4] = {r4.x, r4.y, r4.z, r4.w};
+    uint32_t hn[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) hn[k] = (nb[k] >= 0) ? ldcg(g.height + nb[k]) : UNVIS;
+    const uint32_t h0 = h;
+    const int32_t t0 = t;
+    long long pushed = 0;
+    ++w.visits;
+    for (int step = 0; step < g.local_steps; ++step) {
+        if (t < 0 && h == 1u) {                       // v -> sink (.cu:220-236)
+            const long long cap = -(long long)t;
+            const long long d = ex < cap ? ex : cap;
+            t = (int32_t)((long long)t + d);
+            ex -= d;
+            pushed += d;
+            w.sink += (unsigned long long)d;
+            ++w.pushes;
+        }
+        while (ex > 0) {                               // admissible pushes
+            int best = -1;
+            uint32_t bh = h;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (nb[k] >= 0 && r[k] != 0u && hn[k] < bh) { bh = hn[k]; best = k; }
+            if (best < 0) break;
+            uint32_t rb = 0u;
+            int u = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k == best) { rb = r[k]; u = nb[k]; }
+            const uint32_t d = (uint32_t)(ex < (long long)rb ? ex : (long long)rb);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k == best) r[k] -= d;
+            ex -= d;
+            pushed += d;
+            const uint32_t rk = (rv >> (2 * best)) & 3u;
+            atomicSub(g.res + (size_t)v * 4u + best, d);
+            atomicAdd(g.res + (size_t)u * 4u + rk, d);
+            const unsigned long long old =
+                atomicAdd(reinterpret_cast<unsigned long long*>(g.excess + u), (unsigned long long)d);
+            if (old == 0ull) s_buf[atomicAdd(s_cnt, 1u)] = (uint32_t)u;
+            ++w.pushes;
+        }
+        if (ex <= 0) break;
+        uint32_t mh = (t < 0) ? 0u : UNVIS;            // relabel (.cu:274-301)
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (nb[k] >= 0 && r[k] != 0u && hn[k] < mh) mh = hn[k];
+        ++w.relabels;
+        if (mh == UNVIS) { h = UNVIS; break; }
+        h = mh + 1u;
+        if (h >= n) break;
+    }
+    if (h != h0) g.height[v] = h;
+    if (t != t0) g.term[v] = t;
+    long long now = ex;
+    if (pushed) {
+        const unsigned long long old = atomicAdd(reinterpret_cast<unsigned long long*>(g.excess + v),
+                                                 (unsigned long long)(-pushed));
+        now = (long long)old - pushed;
+    }
+    if (now > 0 && h < n) s_buf[atomicAdd(s_cnt, 1u)] = v;   // keeps ownership
+}
+
+__global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
+{
+    __shared__ uint32_t s_buf[DTPB * 5];
+    __shared__ uint32_t s_cnt, s_n, s_base;
+    __shared__ unsigned long long s_red[DTPB / 32];
+    Ctl* ctl = g.ctl;
+    const uint32_t cnt = ldcg(&ctl->act_cnt[round % 3]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->act_cnt[(round + 2) % 3] = 0u;
+        if (cnt) atomicAdd(&ctl->rounds_done, 1u);
+    }
+    if (cnt == 0) return;
+    const uint32_t* in = (round & 1) ? g.act[1] : g.act[0];
+    uint32_t* out = (round & 1) ? g.act[0] : g.act[1];
+    uint32_t* gcnt = &ctl->act_cnt[(round + 1) % 3];
+    Work w;
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    for (uint32_t base = blockIdx.x * DTPB; base < cnt; base += gridDim.x * DTPB) {
+        const uint32_t i = base + threadIdx.x;
+        if (i < cnt) {
+            const uint32_t v = __ldg(in + i);
+            if (v < g.n) discharge_node(g, v, s_buf, &s_cnt, w);
+            else atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_INVARIANT);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_n = s_cnt;
+            s_cnt = 0;
+            s_base = s_n ? atomicAdd(gcnt, s_n) : 0u;
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < s_n; j += DTPB) out[s_base + j] = s_buf[j];
+        __syncthreads();
+    }
+    unsigned long long x;
+    x = warp_block_sum(w.visits, s_red);
+    if (threadIdx.x == 0 && x) atomicAdd(&ctl->node_visits, x);
+    x = warp_block_sum(w.pushes, s_red);
+    if (threadIdx.x == 0 && x) atomicAdd(&ctl->pushes, x);
+    x = warp_block_sum(w.relabels, s_red);
+    if (threadIdx.x == 0 && x) atomicAdd(&ctl->relabels, x);
+    x = warp_block_sum(w.sink, s_red);
+    if (threadIdx.x == 0 && x) atomicAdd(&ctl->sink_flow, x);
+}
+
+__global__ void __launch_bounds__(DTPB) k_prepare_raw(uint32_t n, const int4* __restrict__ nbr,
+                                                      const uint4* __restrict__ cap,
+                                                      const uint32_t* __restrict__ src,
+                                                      const uint32_t* __restrict__ snk,
+                                                      uint4* __restrict__ res,
+                                                      int32_t* __restrict__ term,
+                                                      unsigned long long* base, int32_t* err)
+{
+    __shared__ unsigned long long s_red[DTPB / 32];
+    unsigned long long b = 0;
+    for (uint32_t v = blockIdx.x * DTPB + threadIdx.x; v < n; v += gridDim.x * DTPB) {
+        const int4 nb = __ldg(nbr + v);
+        uint4 c = __ldg(cap + v);
+        if (nb.x < 0) c.x = 0;
+        if (nb.y < 0) c.y = 0;
+        if (nb.z < 0) c.z = 0;
+        if (nb.w < 0) c.w = 0;
+        if (c.x > 0x7FFFFFFFu || c.y > 0x7FFFFFFFu || c.z > 0x7FFFFFFFu || c.w > 0x7FFFFFFFu)
+            atomicExch(err, 1);
+        res[v] = c;
+        const long long s = __ldg(src + v), k = __ldg(snk + v);
+        const long long d = s - k;
+        if (d < -2147483647LL || d > 2147483647LL) atomicExch(err, 1);
+        term[v] = (int32_t)d;
+        b += (unsigned long long)(s < k ? s : k);
+    }
+    const unsigned long long x = warp_block_sum(b, s_red);
+    if (threadIdx.x == 0 && x) atomicAdd(base, x);
+}
+
+__global__ void k_bounded_wait(const volatile uint32_t* flag, unsigned long long limit_ns,
+                               int32_t* status)
+{
+    unsigned long long t0, t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (;;) {
+        if (*flag != 0u) { *status = 0; return; }
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > limit_ns) { *status = (int32_t)GPUPR_ERR_TIMEOUT; return; }
+        __nanosleep(1000);
+    }
+}
+
+struct PinnedCtl {
+    Ctl* h = nullptr;
+    PinnedCtl() { GPUPR_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h), sizeof(Ctl))); }
+    ~PinnedCtl() { if (h) cudaFreeHost(h); }
+};
+
+Ctl& read_ctl(PinnedCtl& pc, const Ctl* d, cudaStream_t s)
+{
+    GPUPR_CUDA(cudaMemcpyAsync(pc.h, d, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    if (pc.h->error)
+        throw Error{(gpupr_status)pc.h->error,
+                    "GPUPr-B200 device invariant failed code=" + std::to_string(pc.h->error)};
+    return *pc.h;
+}
+
+}  // namespace
+
+int sm_count()
+{
+    static int cached[64] = {0};
+    int dev = 0;
+    GPUPR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cached[dev]) {
+        int v = 0;
+        GPUPR_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        cached[dev] = v > 0 ? v : 1;
+    }
+    return cached[dev];
+}
+
+SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, int period_raw,
+                             uint64_t max_rounds_raw)
+{
+    SolveOptions r;
+    int ls = local_steps_raw;
+    int period = period_raw;
+    uint64_t mr = max_rounds_raw;
+    if (o) {
+        if (o->local_steps) ls = o->local_steps;
+        if (o->global_relabel_period) period = o->global_relabel_period;
+        if (o->max_rounds) mr = o->max_rounds;
+        if (o->time_limit_seconds > 0) r.time_limit_s = o->time_limit_seconds;
+        if (o->round_batch > 0) r.round_batch = o->round_batch;
+        if (o->bfs_batch > 0) r.bfs_batch = o->bfs_batch;
+        if (o->block_size > 0) r.block = o->block_size;
+        if (o->blocks_per_sm > 0) r.blocks_per_sm = o->blocks_per_sm;
+        if (o->work_relabel_factor > 0) r.work_factor = o->work_relabel_factor;
+    }
+    // clamps of gpu_push_relabel_fast.cu:421-424 and :476-480
+    if (ls < 1) ls = 1;
+    if (ls > 32) ls = 32;
+    if (period < 0) period = 0;
+    if (!mr) mr = 2000000ull;
+    r.local_steps = ls;
+    r.relabel_rounds = period > 0 ? ((period + ls - 1) / ls < 1 ? 1 : (period + ls - 1) / ls) : 0;
+    r.max_rounds = mr;
+    return r;
+}
+
+void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const uint8_t* d_rev,
+                        int32_t* d_term, SolveWorkspace& w, const SolveOptions& opt,
+                        cudaStream_t s, SolveResult& out)
+{
+    using Clock = std::chrono::steady_clock;
+    out = SolveResult{};
+    if (!n) return;
+    if (w.excess.n < n) {
+        w.excess = DevBuf<long long>(n, s);
+        w.height = DevBuf<uint32_t>(n, s);
+        w.q0 = DevBuf<uint32_t>(n, s);
+        w.q1 = DevBuf<uint32_t>(n, s);
+        w.q2 = DevBuf<uint32_t>(n, s);
+    }
+    if (!w.ctl.p) w.ctl = DevBuf<Ctl>(1, s);
+    out.workspace_bytes = w.bytes();
+
+    SolveView g{};
+    g.n = n;
+    g.nbr = d_nbr;
+    g.res = d_res;
+    g.rev = d_rev;
+    g.term = d_term;
+    g.excess = w.excess.p;
+    g.height = w.height.p;
+    g.act[0] = w.q0.p;
+    g.act[1] = w.q1.p;
+    g.fr[0] = w.q2.p;
+    g.fr[1] = w.q1.p;   // act[1] is idle while a BFS runs
+    g.ctl = w.ctl.p;
+    g.local_steps = opt.local_steps;
+
+    const int grid = sm_count() * (opt.blocks_per_sm > 0 ? opt.blocks_per_sm : 4);
+    PinnedCtl pc;
+    cudaEvent_t e0, e1, ba, bb;
+    GPUPR_CUDA(cudaEventCreate(&e0));
+    GPUPR_CUDA(cudaEventCreate(&e1));
+    GPUPR_CUDA(cudaEventCreate(&ba));
+    GPUPR_CUDA(cudaEventCreate(&bb));
+    struct EvGuard {
+        cudaEvent_t a, b, c, d;
+        ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); cudaEventDestroy(d); }
+    } evg{e0, e1, ba, bb};
+    // device time of one batch (the host waits for the batch anyway)
+    auto batch_ms = [&]() {
+        float ms = 0.f;
+        GPUPR_CUDA(cudaEventElapsedTime(&ms, ba, bb));
+        return (double)ms;
+    };
+
+    GPUPR_CUDA(cudaMemsetAsync(w.ctl.p, 0, sizeof(Ctl), s));
+    GPUPR_CUDA(cudaEventRecord(e0, s));
+    k_init_excess<<<grid, DTPB, 0, s>>>(n, d_term, w.excess.p);
+    GPUPR_CUDA(cudaGetLastError());
+    out.launches += 1;
+
+    const auto t0 = Clock::now();
+    uint64_t rounds_total = 0;
+    double last_bfs_s = 0.0;
+    for (;;) {
+        // ---- exact global relabel: backward BFS from the sink ----
+        const auto b0 = Clock::now();
+        GPUPR_CUDA(cudaMemsetAsync(w.ctl.p, 0, offsetof(Ctl, error), s));
+        GPUPR_CUDA(cudaEventRecord(ba, s));
+        k_bfs_seed<<<grid, DTPB, 0, s>>>(g);
+        GPUPR_CUDA(cudaGetLastError());
+        out.launches += 1;
+        out.bfs_launches += 1;
+        uint32_t L = 1;
+        for (;;) {
+            for (int b = 0; b < opt.bfs_batch; ++b, ++L) {
+                k_bfs_level<<<grid, DTPB, 0, s>>>(g, L);
+                GPUPR_CUDA(cudaGetLastError());
+            }
+            GPUPR_CUDA(cudaEventRecord(bb, s));
+            out.launches += (uint64_t)opt.bfs_batch;
+            out.bfs_launches += (uint64_t)opt.bfs_batch;
+            const Ctl& hc = read_ctl(pc, w.ctl.p, s);
+            out.bfs_ms += batch_ms();
+            GPUPR_CUDA(cudaEventRecord(ba, s));
+            if (hc.bfs_done) break;
+            if ((uint64_t)L > (uint64_t)n + 2u)
+                throw Error{GPUPR_ERR_INVARIANT, "GPUPr-FAST-v6.30 BFS exceeded n+1 levels"};
+        }
+        ++out.relabels;
+        out.bfs_levels += pc.h->bfs_levels;
+        last_bfs_s = std::chrono::duration<double>(Clock::now() - b0).count();
+        const uint32_t active = pc.h->act_cnt[0];
+        if (active == 0) break;   // maximum preflow: no excess can reach the sink
+        if (rounds_total >= opt.max_rounds)
+            throw Error{GPUPR_ERR_MAX_ROUNDS, "GPUPr-FAST-v6.30 max macro rounds exceeded"};
+
+        // ---- discharge rounds until idle, period or work budget ----
+        const unsigned long long visits0 = pc.h->node_visits;
+        uint32_t r = 0;
+        for (;;) {
+            uint64_t left = opt.max_rounds - rounds_total;
+            int batch = opt.round_batch;
+            if ((uint64_t)batch > left) batch = (int)left;
+            GPUPR_CUDA(cudaEventRecord(ba, s));
+            for (int b = 0; b < batch; ++b, ++r) {
+                k_discharge<<<grid, DTPB, 0, s>>>(g, r);
+                GPUPR_CUDA(cudaGetLastError());
+            }
+            GPUPR_CUDA(cudaEventRecord(bb, s));
+            out.launches += (uint64_t)batch;
+            out.discharge_launches += (uint64_t)batch;
+            const Ctl& hc = read_ctl(pc, w.ctl.p, s);
+            out.discharge_ms += batch_ms();
+            rounds_total = hc.rounds_done;
+            const bool idle = hc.act_cnt[r % 3] == 0u;
+            if (idle) break;
+            if (rounds_total >= opt.max_rounds)
+                throw Error{GPUPR_ERR_MAX_ROUNDS, "GPUPr-FAST-v6.30 max macro rounds exceeded"};
+            if (opt.relabel_rounds > 0 && r >= (uint32_t)opt.relabel_rounds) break;
+            if (opt.work_factor > 0 &&
+                (double)(hc.node_visits - visits0) > opt.work_factor * (double)n)
+                break;
+            const double el = std::chrono::duration<double>(Clock::now() - t0).count();
+            if (el > opt.time_limit_s)
+                throw Error{GPUPR_ERR_TIMEOUT, "GPUPr-FAST-v6.30 solve exceeded 240s safety limit"};
+        }
+    }
+    GPUPR_CUDA(cudaEventRecord(e1, s));
+    GPUPR_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    GPUPR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const Ctl& hc = *pc.h;
+    out.raw_flow = (int64_t)hc.sink_flow;
+    out.rounds = hc.rounds_done;
+    out.node_visits = hc.node_visits;
+    out.pushes = hc.pushes;
+    out.bfs_visits = hc.bfs_visits;
+    out.solve_device_ms = ms;
+    out.final_relabel_s = last_bfs_s;
+    out.solve_s = std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+int64_t prepare_raw_graph(uint32_t n, const uint32_t* d_cap, const uint32_t* d_src,
+                          const uint32_t* d_snk, const int32_t* d_nbr, uint32_t* d_res,
+                          int32_t* d_term, cudaStream_t s, uint64_t* launches)
+{
+    DevBuf<unsigned long long> base(1, s);
+    DevBuf<int32_t> err(1, s);
+    GPUPR_CUDA(cudaMemsetAsync(base.p, 0, sizeof(unsigned long long), s));
+    GPUPR_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int32_t), s));
+    const int grid = sm_count() * 8;
+    k_prepare_raw<<<grid, DTPB, 0, s>>>(n, reinterpret_cast<const int4*>(d_nbr),
+                                        reinterpret_cast<const uint4*>(d_cap), d_src, d_snk,
+                                        reinterpret_cast<uint4*>(d_res), d_term, base.p, err.p);
+    GPUPR_CUDA(cudaGetLastError());
+    *launches += 1;
+    unsigned long long hb = 0;
+    int32_t he = 0;
+    GPUPR_CUDA(cudaMemcpyAsync(&hb, base.p, sizeof(hb), cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaMemcpyAsync(&he, err.p, sizeof(he), cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    if (he) throw Error{GPUPR_ERR_BUILD, "capacity or terminal outside the int32 range"};
+    return (int64_t)hb;
+}
+
+gpupr_status bounded_wait_selftest(uint32_t limit_us, cudaStream_t s)
+{
+    DevBuf<uint32_t> flag(1, s);
+    DevBuf<int32_t> st(1, s);
+    GPUPR_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(uint32_t), s));
+    GPUPR_CUDA(cudaMemsetAsync(st.p, 0xFF, sizeof(int32_t), s));
+    k_bounded_wait<<<1, 1, 0, s>>>(flag.p, (unsigned long long)limit_us * 1000ull, st.p);
+    GPUPR_CUDA(cudaGetLastError());
+    int32_t h = -1;
+    GPUPR_CUDA(cudaMemcpyAsync(&h, st.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    return (gpupr_status)h;
+}
+
+}  // namespace gpupr

@@ -1,0 +1,224 @@
+// pymodule.cpp -- the drop-in `wtivo_gpupr` Python module.
+//
+// Same exports, argument names, defaults, validation order, error text and
+// return tuples as the reference module built from
+// native/gpupr/wtivo_gpupr_bindings.cpp:579-600:
+//   graph_cut_fast(vertices, tets_cuda, neighbors_cuda, labels, fill_T,
+//                  threads=16, global_relabel_period=1024,
+//                  max_rounds=2000000, local_steps=8)        -> 18-tuple
+//   graph_cut_gpupr_fast_v630(...)  (alias)
+//   surface_extraction_topology_cuda(labels, vertices, tets_cuda,
+//                                    neighbors_cuda, threads=16) -> (V, F)
+// PyTorch tensors appear only here: they are inspected through their Python
+// attributes (is_cuda, dtype, shape, data_ptr), so this module links only
+// libwtivo_gpupr.so and never libtorch.  All work goes through the C ABI of
+// include/wtivo_gpupr.h.
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+
+#include <cstdint>
+#include <cstdlib>
+#include <iostream>
+#include <stdexcept>
+#include <string>
+
+#include "wtivo_gpupr.h"
+
+namespace py = pybind11;
+
+namespace {
+
+thread_local gpupr_cut_stats t_last{};
+
+[[noreturn]] void raise_status(gpupr_status st)
+{
+    std::string msg = gpupr_last_error();
+    if (msg.empty()) msg = gpupr_status_string(st);
+    throw std::runtime_error(msg);
+}
+
+bool verbose()
+{
+    const char* v = std::getenv("WTIVO_GPUPR_VERBOSE");
+    return v && v[0] && v[0] != '0';
+}
+
+struct Topo {
+    uintptr_t tets = 0, nbrs = 0;
+    int64_t n = 0;
+    int device = 0;
+};
+
+// bindings.cpp:116-125 (graph cut) / :412-418 (surface, one message)
+Topo check_topology(const py::object& tets, const py::object& nbr, bool surface)
+{
+    py::module_ torch = py::module_::import("torch");
+    py::object Tensor = torch.attr("Tensor");
+    if (!py::isinstance(tets, Tensor) || !py::isinstance(nbr, Tensor))
+        throw py::type_error("tets_cuda and neighbors_cuda must be torch.Tensor objects");
+    const char* smsg = "tets/neighbors must be contiguous CUDA int32 Nx4 with same N";
+    if (!tets.attr("is_cuda").cast<bool>() || !nbr.attr("is_cuda").cast<bool>())
+        throw std::runtime_error(surface ? smsg : "tets/neighbors must be CUDA tensors");
+    py::object i32 = torch.attr("int32");
+    if (!py::object(tets.attr("dtype")).equal(i32) || !py::object(nbr.attr("dtype")).equal(i32))
+        throw std::runtime_error(surface ? smsg : "tets/neighbors must be int32");
+    if (!tets.attr("is_contiguous")().cast<bool>() || !nbr.attr("is_contiguous")().cast<bool>())
+        throw std::runtime_error(surface ? smsg : "tets/neighbors must be contiguous");
+    if (tets.attr("dim")().cast<int64_t>() != 2 || nbr.attr("dim")().cast<int64_t>() != 2 ||
+        tets.attr("size")(1).cast<int64_t>() != 4 || nbr.attr("size")(1).cast<int64_t>() != 4 ||
+        tets.attr("size")(0).cast<int64_t>() != nbr.attr("size")(0).cast<int64_t>())
+        throw std::runtime_error(surface ? smsg : "tets/neighbors must be Nx4 and same N");
+    Topo t;
+    t.n = tets.attr("size")(0).cast<int64_t>();
+    t.tets = tets.attr("data_ptr")().cast<uintptr_t>();
+    t.nbrs = nbr.attr("data_ptr")().cast<uintptr_t>();
+    t.device = tets.attr("device").attr("index").cast<int>();
+    return t;
+}
+
+void* current_stream(int device)
+{
+    py::module_ torch = py::module_::import("torch");
+    py::object s = torch.attr("cuda").attr("current_stream")(device);
+    return reinterpret_cast<void*>(s.attr("cuda_stream").cast<uintptr_t>());
+}
+
+using F64 = py::array_t<double, py::array::c_style | py::array::forcecast>;
+using U8 = py::array_t<std::uint8_t, py::array::c_style | py::array::forcecast>;
+
+py::tuple graph_cut_fast(F64 vertices, py::object tets_cuda, py::object nbr_cuda, U8 labels,
+                         double fill_T, int threads, int global_relabel_period,
+                         std::uint64_t max_rounds, int local_steps)
+{
+    // bindings.cpp:114-132, in the same order
+    if (vertices.ndim() != 2 || vertices.shape(1) != 3)
+        throw std::runtime_error("vertices must be float64 Nx3");
+    const Topo t = check_topology(tets_cuda, nbr_cuda, false);
+    const std::uint64_t N = static_cast<std::uint64_t>(t.n);
+    if (labels.ndim() != 1 || static_cast<std::uint64_t>(labels.shape(0)) != N)
+        throw std::runtime_error("labels size mismatch");
+    if (N > 0xFFFFFFFFull) throw std::runtime_error(">2^32 full tets unsupported");
+    const std::uint64_t nv = static_cast<std::uint64_t>(vertices.shape(0));
+    void* stream = current_stream(t.device);
+    py::array_t<std::uint8_t> out(static_cast<py::ssize_t>(N));
+    gpupr_cut_stats st{};
+    gpupr_status rc;
+    {
+        py::gil_scoped_release nogil;
+        rc = gpupr_graph_cut(vertices.data(), nv, 0, reinterpret_cast<const std::int32_t*>(t.tets),
+                             reinterpret_cast<const std::int32_t*>(t.nbrs), N, labels.data(), 0,
+                             fill_T, threads, global_relabel_period, max_rounds, local_steps,
+                             out.mutable_data(), 0, stream, &st);
+    }
+    if (rc != GPUPR_OK) raise_status(rc);
+    t_last = st;
+    if (N && st.free_n == 0) {
+        // bindings.cpp:191-196: the reference's 16-tuple early return
+        return py::make_tuple(out, 0, 0, 0, 0, py::int_(st.full_E), 0, py::int_(st.fixed_source),
+                              py::int_(st.fixed_sink), 0, py::int_(st.threads), 0, 0, 0, 0.0,
+                              py::int_(st.local_steps));
+    }
+    if (N == 0) {
+        return py::make_tuple(out, 0, 0, 0, 0, 0, 0, 0, 0, 0, py::int_(st.threads), 0, 0, 0, 0.0,
+                              py::int_(st.local_steps));
+    }
+    if (verbose()) {
+        std::cout << "[GPUPr-B200] build=" << st.build_seconds << "s | free nodes=" << st.free_n
+                  << " | solve=" << st.solve_seconds << "s | rounds=" << st.rounds
+                  << " | global_relabels=" << st.global_relabels
+                  << " | final_relabel=" << st.final_relabel_seconds
+                  << "s | flow=" << st.adjusted_flow << std::endl;
+    }
+    return py::make_tuple(out, py::int_(st.adjusted_flow), py::int_(st.raw_flow),
+                          py::int_(st.graph_bytes), py::int_(st.workspace_bytes),
+                          py::int_(st.full_E), py::int_(st.free_E), py::int_(st.fixed_source),
+                          py::int_(st.fixed_sink), py::int_(st.terminal_edges),
+                          py::int_(st.threads), py::int_(st.rounds),
+                          py::int_(st.global_relabels), py::int_(st.map_bytes),
+                          py::float_(st.build_seconds), py::int_(st.local_steps),
+                          py::float_(st.solve_seconds), py::float_(st.native_total_seconds));
+}
+
+py::tuple surface_extraction_topology_cuda(U8 labels, F64 vertices, py::object tets_cuda,
+                                           py::object nbr_cuda, int threads)
+{
+    (void)threads;  // the order does not depend on it (bindings.cpp:469-470)
+    if (vertices.ndim() != 2 || vertices.shape(1) != 3)
+        throw std::runtime_error("vertices must be float64 Nx3");
+    const Topo t = check_topology(tets_cuda, nbr_cuda, true);
+    const std::uint64_t N = static_cast<std::uint64_t>(t.n);
+    if (labels.ndim() != 1 || static_cast<std::uint64_t>(labels.shape(0)) != N)
+        throw std::runtime_error("labels size mismatch");
+    const std::uint64_t nv = static_cast<std::uint64_t>(vertices.shape(0));
+    void* stream = current_stream(t.device);
+    std::uint64_t nf = 0, nu = 0;
+    gpupr_status rc;
+    {
+        py::gil_scoped_release nogil;
+        rc = gpupr_surface_count(labels.data(), 0, vertices.data(), nv, 0,
+                                 reinterpret_cast<const std::int32_t*>(t.tets),
+                                 reinterpret_cast<const std::int32_t*>(t.nbrs), N, &nf, &nu, stream);
+    }
+    if (rc != GPUPR_OK) raise_status(rc);
+    py::array_t<double> OV({static_cast<py::ssize_t>(nu), py::ssize_t(3)});
+    py::array_t<std::int32_t> OF({static_cast<py::ssize_t>(nf), py::ssize_t(3)});
+    {
+        py::gil_scoped_release nogil;
+        rc = gpupr_surface_fetch(OF.mutable_data(), OV.mutable_data(), 0, stream);
+    }
+    if (rc != GPUPR_OK) raise_status(rc);
+    return py::make_tuple(OV, OF);
+}
+
+py::dict last_stats()
+{
+    const gpupr_cut_stats& s = t_last;
+    py::dict d;
+    d["adjusted_flow"] = s.adjusted_flow;
+    d["raw_flow"] = s.raw_flow;
+    d["graph_bytes"] = s.graph_bytes;
+    d["workspace_bytes"] = s.workspace_bytes;
+    d["free_n"] = s.free_n;
+    d["n_full"] = s.n_full;
+    d["rounds"] = s.rounds;
+    d["global_relabels"] = s.global_relabels;
+    d["build_seconds"] = s.build_seconds;
+    d["solve_seconds"] = s.solve_seconds;
+    d["final_relabel_seconds"] = s.final_relabel_seconds;
+    d["partition_seconds"] = s.partition_seconds;
+    d["native_total_seconds"] = s.native_total_seconds;
+    d["node_visits"] = s.node_visits;
+    d["pushes"] = s.pushes;
+    d["bfs_visits"] = s.bfs_visits;
+    d["bfs_levels"] = s.bfs_levels;
+    d["kernel_launches"] = s.kernel_launches;
+    d["solve_device_ms"] = s.solve_device_ms;
+    d["build_device_ms"] = s.build_device_ms;
+    return d;
+}
+
+}  // namespace
+
+PYBIND11_MODULE(wtivo_gpupr, m)
+{
+    m.doc() = "WTiVo graph cut on B200: GPU reduced-graph build, multi-discharge push-relabel "
+              "with exact global relabels, and GPU cut-surface extraction";
+    m.def("graph_cut_fast", &graph_cut_fast, py::arg("vertices"), py::arg("tets_cuda"),
+          py::arg("neighbors_cuda"), py::arg("labels"), py::arg("fill_T"), py::arg("threads") = 16,
+          py::arg("global_relabel_period") = 1024, py::arg("max_rounds") = 2000000ULL,
+          py::arg("local_steps") = 8);
+    m.def("graph_cut_gpupr_fast_v630", &graph_cut_fast, py::arg("vertices"), py::arg("tets_cuda"),
+          py::arg("neighbors_cuda"), py::arg("labels"), py::arg("fill_T"), py::arg("threads") = 16,
+          py::arg("global_relabel_period") = 1024, py::arg("max_rounds") = 2000000ULL,
+          py::arg("local_steps") = 8);
+    m.def("surface_extraction_topology_cuda", &surface_extraction_topology_cuda, py::arg("labels"),
+          py::arg("vertices"), py::arg("tets_cuda"), py::arg("neighbors_cuda"),
+          py::arg("threads") = 16);
+    m.def("last_stats", &last_stats,
+          "Extended statistics of the last graph_cut_fast call on this thread.");
+    m.def("release_cached_memory", []() {
+        const gpupr_status rc = gpupr_release_cached_memory();
+        if (rc != GPUPR_OK) raise_status(rc);
+    });
+    m.attr("abi_version") = gpupr_abi_version();
+}

@@ -1,0 +1,262 @@
+"""ctypes front end of ``libwtivo_gpupr.so`` (the C ABI in include/wtivo_gpupr.h).
+
+Device buffers are passed as torch CUDA tensors (their data_ptr) and host
+buffers as numpy arrays; torch is only used for device memory and streams.
+Every call raises ``GpuprError`` with the library's message on failure.
+The CUDA library is required: loading fails loudly if it is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libwtivo_gpupr.so"
+HEADER = PKG.parent / "include" / "wtivo_gpupr.h"
+
+STATS_FIELDS = [
+    ("adjusted_flow", ctypes.c_int64), ("raw_flow", ctypes.c_int64),
+    ("graph_bytes", ctypes.c_uint64), ("workspace_bytes", ctypes.c_uint64),
+    ("full_E", ctypes.c_uint64), ("free_E", ctypes.c_uint64),
+    ("fixed_source", ctypes.c_uint64), ("fixed_sink", ctypes.c_uint64),
+    ("terminal_edges", ctypes.c_uint64), ("threads", ctypes.c_int64),
+    ("rounds", ctypes.c_uint64), ("global_relabels", ctypes.c_uint64),
+    ("map_bytes", ctypes.c_uint64), ("build_seconds", ctypes.c_double),
+    ("local_steps", ctypes.c_int64), ("solve_seconds", ctypes.c_double),
+    ("native_total_seconds", ctypes.c_double),
+    ("free_n", ctypes.c_uint64), ("n_full", ctypes.c_uint64),
+    ("final_relabel_seconds", ctypes.c_double), ("partition_seconds", ctypes.c_double),
+    ("node_visits", ctypes.c_uint64), ("pushes", ctypes.c_uint64),
+    ("bfs_visits", ctypes.c_uint64), ("bfs_levels", ctypes.c_uint64),
+    ("kernel_launches", ctypes.c_uint64), ("solve_device_ms", ctypes.c_double),
+    ("build_device_ms", ctypes.c_double), ("discharge_ms", ctypes.c_double),
+    ("bfs_ms", ctypes.c_double), ("discharge_launches", ctypes.c_uint64),
+    ("bfs_launches", ctypes.c_uint64),
+]
+
+
+class CutStats(ctypes.Structure):
+    _fields_ = STATS_FIELDS
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SolveOptions(ctypes.Structure):
+    _fields_ = [
+        ("local_steps", ctypes.c_int32), ("global_relabel_period", ctypes.c_int32),
+        ("max_rounds", ctypes.c_uint64), ("time_limit_seconds", ctypes.c_double),
+        ("round_batch", ctypes.c_int32), ("bfs_batch", ctypes.c_int32),
+        ("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+        ("work_relabel_factor", ctypes.c_double),
+    ]
+
+
+class GpuprError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+STATUS = {
+    0: "GPUPR_OK", 1: "GPUPR_ERR_INVALID_ARGUMENT", 2: "GPUPR_ERR_NEIGHBOR_RANGE",
+    3: "GPUPR_ERR_REFS_ODD", 4: "GPUPR_ERR_BUILD", 5: "GPUPR_ERR_FREE_REFS_ODD",
+    6: "GPUPR_ERR_TOO_MANY_NODES", 7: "GPUPR_ERR_NO_REVERSE", 8: "GPUPR_ERR_OUT_OF_MEMORY",
+    9: "GPUPR_ERR_MAX_ROUNDS", 10: "GPUPR_ERR_INVARIANT", 11: "GPUPR_ERR_CUDA",
+    12: "GPUPR_ERR_TIMEOUT", 13: "GPUPR_ERR_TOO_MANY_TETS",
+}
+
+_lib = None
+
+
+def header_functions():
+    """Names of every function the public header declares."""
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(gpupr_[a-z_0-9]+)\s*\(",
+                                 text, flags=re.M)))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is not built; run build.py (no CPU fallback exists)")
+        L = ctypes.CDLL(str(LIB_PATH))
+        p, u64, i32, f64 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_double
+        L.gpupr_status_string.restype = ctypes.c_char_p
+        L.gpupr_status_string.argtypes = [ctypes.c_int]
+        L.gpupr_last_error.restype = ctypes.c_char_p
+        L.gpupr_last_error.argtypes = []
+        L.gpupr_abi_version.restype = ctypes.c_int
+        L.gpupr_graph_cut.argtypes = [p, u64, ctypes.c_int, p, p, u64, p, ctypes.c_int, f64, i32,
+                                      i32, u64, i32, p, ctypes.c_int, p, p]
+        L.gpupr_graph_cut_ex.argtypes = [p, u64, ctypes.c_int, p, p, u64, p, ctypes.c_int, f64,
+                                         i32, p, p, ctypes.c_int, p, p]
+        L.gpupr_build_reduced.argtypes = [p, u64, ctypes.c_int, p, p, u64, p, ctypes.c_int, f64,
+                                          p, p, p, p, p, p, p, p]
+        L.gpupr_solve_reduced.argtypes = [ctypes.c_uint32, p, p, p, p, i32, u64, i32, p, p, p]
+        L.gpupr_solve_ell.argtypes = [ctypes.c_uint32, p, p, p, p, p, p, p, p, p]
+        L.gpupr_surface_count.argtypes = [p, ctypes.c_int, p, u64, ctypes.c_int, p, p, u64, p, p, p]
+        L.gpupr_surface_fetch.argtypes = [p, p, ctypes.c_int, p]
+        L.gpupr_release_cached_memory.argtypes = []
+        L.gpupr_selftest_bounded_wait.argtypes = [ctypes.c_uint32, p]
+        for name in header_functions():
+            fn = getattr(L, name)
+            if name not in ("gpupr_status_string", "gpupr_last_error", "gpupr_abi_version"):
+                fn.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        msg = lib().gpupr_last_error().decode() or lib().gpupr_status_string(rc).decode()
+        raise GpuprError(rc, msg)
+
+
+def _dp(t):
+    """device pointer of a torch CUDA tensor"""
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _hp(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _stream(torch, device=None):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def options(**kw):
+    o = SolveOptions()
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def graph_cut(vertices, tets, nbrs, labels, fill_T, threads=16, global_relabel_period=1024,
+              max_rounds=2000000, local_steps=8, opts=None, out=None):
+    """gpupr_graph_cut(_ex).  ``tets``/``nbrs`` are CUDA int32 tensors.
+    ``vertices``/``labels`` may be numpy arrays (host) or CUDA tensors.
+    Returns (labels_out, stats dict); labels_out matches ``out`` placement
+    (a new numpy array when out is None and labels are on the host)."""
+    import torch
+
+    v_dev = isinstance(vertices, torch.Tensor)
+    l_dev = isinstance(labels, torch.Tensor)
+    N = int(tets.shape[0])
+    if out is None:
+        out = torch.empty(N, dtype=torch.uint8, device=tets.device) if l_dev else np.empty(N, np.uint8)
+    o_dev = isinstance(out, torch.Tensor)
+    if v_dev:
+        vp = _dp(vertices)
+    else:
+        vertices = np.ascontiguousarray(vertices, np.float64)
+        vp = _hp(vertices)
+    if not l_dev:
+        labels = np.ascontiguousarray(labels, np.uint8)
+    lp = _dp(labels) if l_dev else _hp(labels)
+    op = _dp(out) if o_dev else _hp(out)
+    st = CutStats()
+    nv = int(vertices.shape[0])
+    if opts is None:
+        rc = lib().gpupr_graph_cut(vp, nv, int(v_dev), _dp(tets), _dp(nbrs), N, lp, int(l_dev),
+                                   float(fill_T), int(threads), int(global_relabel_period),
+                                   int(max_rounds), int(local_steps), op, int(o_dev),
+                                   _stream(torch, tets.device), ctypes.byref(st))
+    else:
+        rc = lib().gpupr_graph_cut_ex(vp, nv, int(v_dev), _dp(tets), _dp(nbrs), N, lp, int(l_dev),
+                                      float(fill_T), int(threads), ctypes.byref(opts), op,
+                                      int(o_dev), _stream(torch, tets.device), ctypes.byref(st))
+    check(rc)
+    return out, st.as_dict()
+
+
+def build_reduced(vertices, tets, nbrs, labels, fill_T):
+    """gpupr_build_reduced: the reduced graph copied back to the host."""
+    import torch
+
+    vertices = np.ascontiguousarray(vertices, np.float64)
+    labels = np.ascontiguousarray(labels, np.uint8)
+    N = int(tets.shape[0])
+    f2f = np.empty(max(N, 1), np.int32)
+    old = np.empty(max(N, 1), np.uint32)
+    nbr = np.empty((max(N, 1), 4), np.int32)
+    res = np.empty((max(N, 1), 4), np.uint32)
+    term = np.empty(max(N, 1), np.int32)
+    rev = np.empty(max(N, 1), np.uint8)
+    info = np.zeros(8, np.int64)
+    check(lib().gpupr_build_reduced(_hp(vertices), vertices.shape[0], 0, _dp(tets), _dp(nbrs), N,
+                                    _hp(labels), 0, float(fill_T), _hp(f2f), _hp(old), _hp(nbr),
+                                    _hp(res), _hp(term), _hp(rev), _hp(info),
+                                    _stream(torch, tets.device)))
+    F = int(info[0])
+    keys = ("free_n", "fixed_source", "fixed_sink", "full_refs", "free_refs", "terminal_edges",
+            "terminal_base_flow", "n_full")
+    return dict(full_to_free=f2f[:N], free_old=old[:F], nbr=nbr[:F], res=res[:F], term=term[:F],
+                rev=rev[:F], info={k: int(v) for k, v in zip(keys, info)})
+
+
+def solve_reduced(nbr, res, term, local_steps=8, global_relabel_period=1024, max_rounds=2000000,
+                  want_excess=False):
+    """gpupr_solve_reduced on CUDA tensors nbr int32[n,4], res int32/uint32
+    [n,4], term int32[n] (modified in place).  Returns (partition numpy,
+    stats, excess tensor or None)."""
+    import torch
+
+    n = int(nbr.shape[0])
+    part = np.zeros(max(n, 1), np.uint8)
+    exc = torch.zeros(max(n, 1), dtype=torch.int64, device=nbr.device) if want_excess else None
+    st = CutStats()
+    check(lib().gpupr_solve_reduced(n, _dp(nbr), _dp(res), _dp(term), _hp(part),
+                                    int(global_relabel_period), int(max_rounds), int(local_steps),
+                                    _dp(exc) if exc is not None else None,
+                                    _stream(torch, nbr.device), ctypes.byref(st)))
+    return part[:n], st.as_dict(), exc
+
+
+def solve_ell(nbr, cap, src, snk, opts=None):
+    """gpupr_solve_ell on CUDA tensors.  Returns (max_flow, partition tensor,
+    stats)."""
+    import torch
+
+    n = int(nbr.shape[0])
+    part = torch.empty(max(n, 1), dtype=torch.uint8, device=nbr.device)
+    flow = ctypes.c_int64(0)
+    st = CutStats()
+    check(lib().gpupr_solve_ell(n, _dp(nbr), _dp(cap), _dp(src), _dp(snk),
+                                ctypes.byref(opts) if opts is not None else None,
+                                ctypes.byref(flow), _dp(part), _stream(torch, nbr.device),
+                                ctypes.byref(st)))
+    return int(flow.value), part[:n], st.as_dict()
+
+
+def surface(labels, vertices, tets, nbrs):
+    """gpupr_surface_count + fetch with host labels/vertices -> (V, F)."""
+    import torch
+
+    labels = np.ascontiguousarray(labels, np.uint8)
+    vertices = np.ascontiguousarray(vertices, np.float64)
+    nf = ctypes.c_uint64(0)
+    nu = ctypes.c_uint64(0)
+    s = _stream(torch, tets.device)
+    check(lib().gpupr_surface_count(_hp(labels), 0, _hp(vertices), vertices.shape[0], 0, _dp(tets),
+                                    _dp(nbrs), int(tets.shape[0]), ctypes.byref(nf),
+                                    ctypes.byref(nu), s))
+    F = np.empty((max(nf.value, 1), 3), np.int32)
+    V = np.empty((max(nu.value, 1), 3), np.float64)
+    check(lib().gpupr_surface_fetch(_hp(F), _hp(V), 0, s))
+    return V[: nu.value], F[: nf.value]
+
+
+def bounded_wait_selftest(limit_us=200_000):
+    import torch
+
+    return lib().gpupr_selftest_bounded_wait(int(limit_us), _stream(torch))
+
+
+def release_cached_memory():
+    check(lib().gpupr_release_cached_memory())

@@ -1,0 +1,335 @@
+/*
+ * synth.c -- seeded synthetic inputs for the graph-cut path.
+ *
+ * The reference produces its cell graph with CGAL (Delaunay of a point
+ * proxy, native/core/wtivo_core.cpp:72-165) and its tet labels with an
+ * OpenVDB unsigned-distance field sampled at tet centroids
+ * (native/vdb/wtivo_vdb.cpp:1519-1584).  Neither library exists here, so
+ * these host routines stand in for them:
+ *
+ *  - synth_lattice: a jittered Kuhn (Freudenthal) tetrahedralization of a
+ *    box, 6 tets per cube, with neighbors computed analytically in the
+ *    reference's CelloCut slot convention (slot fi shares face
+ *    {012,013,023,123}[fi], i.e. the tet opposite local vertex 3-fi;
+ *    -1 on the hull).  Cubes are emitted in Morton order so that tet ids are
+ *    spatially coherent, as CGAL's spatially sorted insertion makes them.
+ *  - synth_udf_labels: label 0 iff the exact point-to-triangle distance from
+ *    a tet centroid (mean of its 4 vertices, as wtivo_vdb.cpp:1561-1570) to
+ *    the mesh is <= threshold, else 1 (wtivo_vdb.cpp:1577-1578).  Centroids
+ *    and mesh may be given separate affine maps so the reference's label
+ *    query coordinates can be mimicked.
+ *
+ * Everything is deterministic for a given seed (hash-based jitter) and
+ * independent of the thread count.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+static inline uint64_t mix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+static inline double u01(uint64_t h) { return (double)(h >> 11) * (1.0 / 9007199254740992.0); }
+
+/* permutations of the axes; tet p of a cube walks e[P[p][0]], e[P[p][1]],
+ * e[P[p][2]] from the cube's low corner to its high corner. */
+static const int PERM[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+
+static int perm_index(int a, int b, int c)
+{
+    for (int p = 0; p < 6; ++p)
+        if (PERM[p][0] == a && PERM[p][1] == b && PERM[p][2] == c) return p;
+    return -1;
+}
+
+static inline uint64_t spread3(uint64_t v)
+{
+    v &= 0x1FFFFFull;
+    v = (v | (v << 32)) & 0x1F00000000FFFFull;
+    v = (v | (v << 16)) & 0x1F0000FF0000FFull;
+    v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+    v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+static inline uint32_t compact3(uint64_t v)
+{
+    v &= 0x1249249249249249ull;
+    v = (v ^ (v >> 2)) & 0x10C30C30C30C30C3ull;
+    v = (v ^ (v >> 4)) & 0x100F00F00F00F00Full;
+    v = (v ^ (v >> 8)) & 0x1F0000FF0000FFull;
+    v = (v ^ (v >> 16)) & 0x1F00000000FFFFull;
+    v = (v ^ (v >> 32)) & 0x1FFFFFull;
+    return (uint32_t)v;
+}
+
+/* Returns the number of tets (6*nx*ny*nz) or -1 on bad arguments.
+ * V[(nx+1)(ny+1)(nz+1)*3], tets/nbrs[6*nx*ny*nz*4],
+ * cube_rank scratch[nx*ny*nz]. jitter is a fraction of the cell size. */
+int64_t synth_lattice(int nx, int ny, int nz, const double* lo, const double* h,
+                      double jitter, uint64_t seed, double* V, int32_t* tets,
+                      int32_t* nbrs, int32_t* cube_rank)
+{
+    if (nx < 1 || ny < 1 || nz < 1) return -1;
+    const int64_t ncube = (int64_t)nx * ny * nz;
+    if (ncube * 6 > 0x7FFFFFFFll) return -1;
+    const int64_t vx = nx + 1, vy = ny + 1, vz = nz + 1;
+
+#pragma omp parallel for schedule(static)
+    for (int64_t z = 0; z < vz; ++z)
+        for (int64_t y = 0; y < vy; ++y)
+            for (int64_t x = 0; x < vx; ++x) {
+                const int64_t id = x + vx * (y + vy * z);
+                const uint64_t hs = mix64(seed ^ mix64((uint64_t)id));
+                double j[3];
+                j[0] = (u01(hs) - 0.5) * 2.0 * jitter;
+                j[1] = (u01(mix64(hs + 1)) - 0.5) * 2.0 * jitter;
+                j[2] = (u01(mix64(hs + 2)) - 0.5) * 2.0 * jitter;
+                /* boundary vertices stay on the box faces */
+                if (x == 0 || x == vx - 1) j[0] = 0.0;
+                if (y == 0 || y == vy - 1) j[1] = 0.0;
+                if (z == 0 || z == vz - 1) j[2] = 0.0;
+                V[id * 3 + 0] = lo[0] + ((double)x + j[0]) * h[0];
+                V[id * 3 + 1] = lo[1] + ((double)y + j[1]) * h[1];
+                V[id * 3 + 2] = lo[2] + ((double)z + j[2]) * h[2];
+            }
+
+    /* Morton ranks of the cubes */
+    int bits = 0;
+    while ((1 << bits) < nx || (1 << bits) < ny || (1 << bits) < nz) ++bits;
+    const uint64_t codes = 1ull << (3 * bits);
+    int64_t rank = 0;
+    for (uint64_t m = 0; m < codes; ++m) {
+        const uint32_t x = compact3(m), y = compact3(m >> 1), z = compact3(m >> 2);
+        if ((int)x >= nx || (int)y >= ny || (int)z >= nz) continue;
+        cube_rank[x + (int64_t)nx * (y + (int64_t)ny * z)] = (int32_t)rank++;
+    }
+
+#pragma omp parallel for schedule(static)
+    for (int64_t z = 0; z < nz; ++z)
+        for (int64_t y = 0; y < ny; ++y)
+            for (int64_t x = 0; x < nx; ++x) {
+                const int64_t c = x + nx * (y + ny * z);
+                const int64_t r = cube_rank[c];
+                for (int p = 0; p < 6; ++p) {
+                    const int64_t t = r * 6 + p;
+                    int64_t cur[3] = {x, y, z};
+                    int32_t vid[4];
+                    for (int k = 0; k < 4; ++k) {
+                        if (k > 0) cur[PERM[p][k - 1]] += 1;
+                        vid[k] = (int32_t)(cur[0] + vx * (cur[1] + vy * cur[2]));
+                    }
+                    for (int k = 0; k < 4; ++k) tets[t * 4 + k] = vid[k];
+                    const int a = PERM[p][0], b = PERM[p][1], cc = PERM[p][2];
+                    /* slot 0: face opposite v3 -> cube - e_c, perm (c,a,b) */
+                    {
+                        int64_t q[3] = {x, y, z};
+                        q[cc] -= 1;
+                        int32_t nb = -1;
+                        if (q[0] >= 0 && q[1] >= 0 && q[2] >= 0) {
+                            const int64_t qc = q[0] + nx * (q[1] + ny * q[2]);
+                            nb = (int32_t)((int64_t)cube_rank[qc] * 6 + perm_index(cc, a, b));
+                        }
+                        nbrs[t * 4 + 0] = nb;
+                    }
+                    /* slot 1: face opposite v2 -> same cube, perm (a,c,b) */
+                    nbrs[t * 4 + 1] = (int32_t)(r * 6 + perm_index(a, cc, b));
+                    /* slot 2: face opposite v1 -> same cube, perm (b,a,c) */
+                    nbrs[t * 4 + 2] = (int32_t)(r * 6 + perm_index(b, a, cc));
+                    /* slot 3: face opposite v0 -> cube + e_a, perm (b,c,a) */
+                    {
+                        int64_t q[3] = {x, y, z};
+                        q[a] += 1;
+                        int32_t nb = -1;
+                        if (q[0] < nx && q[1] < ny && q[2] < nz) {
+                            const int64_t qc = q[0] + nx * (q[1] + ny * q[2]);
+                            nb = (int32_t)((int64_t)cube_rank[qc] * 6 + perm_index(b, cc, a));
+                        }
+                        nbrs[t * 4 + 3] = nb;
+                    }
+                }
+            }
+    return ncube * 6;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Exact point-to-triangle squared distance (closest point by region,      */
+/* C. Ericson, Real-Time Collision Detection, 2005, sec. 5.1.5).           */
+/* ---------------------------------------------------------------------- */
+static double pt_tri_d2(const double* p, const double* a, const double* b, const double* c)
+{
+    double ab[3], ac[3], ap[3];
+    for (int i = 0; i < 3; ++i) { ab[i] = b[i] - a[i]; ac[i] = c[i] - a[i]; ap[i] = p[i] - a[i]; }
+    const double d1 = ab[0] * ap[0] + ab[1] * ap[1] + ab[2] * ap[2];
+    const double d2 = ac[0] * ap[0] + ac[1] * ap[1] + ac[2] * ap[2];
+    double q[3];
+    if (d1 <= 0.0 && d2 <= 0.0) { memcpy(q, a, sizeof q); goto out; }
+    double bp[3];
+    for (int i = 0; i < 3; ++i) bp[i] = p[i] - b[i];
+    const double d3 = ab[0] * bp[0] + ab[1] * bp[1] + ab[2] * bp[2];
+    const double d4 = ac[0] * bp[0] + ac[1] * bp[1] + ac[2] * bp[2];
+    if (d3 >= 0.0 && d4 <= d3) { memcpy(q, b, sizeof q); goto out; }
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+        const double v = d1 / (d1 - d3);
+        for (int i = 0; i < 3; ++i) q[i] = a[i] + v * ab[i];
+        goto out;
+    }
+    double cp[3];
+    for (int i = 0; i < 3; ++i) cp[i] = p[i] - c[i];
+    const double d5 = ab[0] * cp[0] + ab[1] * cp[1] + ab[2] * cp[2];
+    const double d6 = ac[0] * cp[0] + ac[1] * cp[1] + ac[2] * cp[2];
+    if (d6 >= 0.0 && d5 <= d6) { memcpy(q, c, sizeof q); goto out; }
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+        const double w = d2 / (d2 - d6);
+        for (int i = 0; i < 3; ++i) q[i] = a[i] + w * ac[i];
+        goto out;
+    }
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+        const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        for (int i = 0; i < 3; ++i) q[i] = b[i] + w * (c[i] - b[i]);
+        goto out;
+    }
+    {
+        const double denom = 1.0 / (va + vb + vc);
+        const double v = vb * denom, w = vc * denom;
+        for (int i = 0; i < 3; ++i) q[i] = a[i] + ab[i] * v + ac[i] * w;
+    }
+out:;
+    const double dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
+    return dx * dx + dy * dy + dz * dz;
+}
+
+/* Label tets by the unsigned distance of their centroid to a triangle mesh.
+ * Centroid c (tet-vertex space) is mapped to query space by q = c*cs + co
+ * per axis; mesh vertices are mapped by m = v*ms + mo.  labels[i] = 0 iff
+ * dist(q, mesh) <= threshold.  Returns 0, or -1 on bad input. */
+int synth_udf_labels(const double* V, int64_t nv, const int32_t* tets, int64_t N,
+                     const double* cs, const double* co,
+                     const double* TV, int64_t ntv, const int32_t* TF, int64_t ntf,
+                     const double* ms, const double* mo,
+                     double threshold, uint8_t* labels)
+{
+    if (ntf <= 0) { memset(labels, 1, (size_t)N); return 0; }
+    double* MV = (double*)malloc((size_t)ntv * 3 * sizeof(double));
+    if (!MV) return -1;
+    double bmin[3] = {1e300, 1e300, 1e300}, bmax[3] = {-1e300, -1e300, -1e300};
+    for (int64_t i = 0; i < ntv; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const double m = TV[i * 3 + k] * ms[k] + mo[k];
+            MV[i * 3 + k] = m;
+            if (m < bmin[k]) bmin[k] = m;
+            if (m > bmax[k]) bmax[k] = m;
+        }
+    /* grid over the threshold-expanded bbox; cell >= threshold */
+    double span = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        bmin[k] -= threshold;
+        bmax[k] += threshold;
+        if (bmax[k] - bmin[k] > span) span = bmax[k] - bmin[k];
+    }
+    double cell = span / 256.0;
+    if (cell < threshold) cell = threshold;
+    /* mean edge length keeps the triangle-per-cell fan-out small */
+    double el = 0.0;
+    int64_t nel = 0;
+    const int64_t estep = ntf / 4096 + 1;
+    for (int64_t f = 0; f < ntf; f += estep, ++nel) {
+        const double* a = MV + (size_t)TF[f * 3] * 3;
+        const double* b = MV + (size_t)TF[f * 3 + 1] * 3;
+        el += sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+    }
+    el /= (double)nel;
+    if (cell < el) cell = el;
+    int dim[3];
+    for (int k = 0; k < 3; ++k) {
+        dim[k] = (int)((bmax[k] - bmin[k]) / cell) + 1;
+        if (dim[k] > 512) dim[k] = 512;
+    }
+    double inv[3];
+    for (int k = 0; k < 3; ++k) inv[k] = (double)dim[k] / (bmax[k] - bmin[k]);
+    const int64_t ncell = (int64_t)dim[0] * dim[1] * dim[2];
+    int64_t* off = (int64_t*)calloc((size_t)ncell + 1, sizeof(int64_t));
+    if (!off) { free(MV); return -1; }
+    for (int pass = 0; pass < 2; ++pass) {
+        int32_t* list = NULL;
+        int64_t* fill = NULL;
+        if (pass == 1) {
+            for (int64_t c = 0; c < ncell; ++c) off[c + 1] += off[c];
+            list = (int32_t*)malloc((size_t)off[ncell] * sizeof(int32_t) + 4);
+            fill = (int64_t*)malloc((size_t)ncell * sizeof(int64_t));
+            if (!list || !fill) { free(list); free(fill); free(off); free(MV); return -1; }
+            memcpy(fill, off, (size_t)ncell * sizeof(int64_t));
+        }
+        for (int64_t f = 0; f < ntf; ++f) {
+            int lo3[3], hi3[3];
+            for (int k = 0; k < 3; ++k) {
+                double mn = 1e300, mx = -1e300;
+                for (int j = 0; j < 3; ++j) {
+                    const double m = MV[(size_t)TF[f * 3 + j] * 3 + k];
+                    if (m < mn) mn = m;
+                    if (m > mx) mx = m;
+                }
+                lo3[k] = (int)floor((mn - threshold - bmin[k]) * inv[k]);
+                hi3[k] = (int)floor((mx + threshold - bmin[k]) * inv[k]);
+                if (lo3[k] < 0) lo3[k] = 0;
+                if (hi3[k] >= dim[k]) hi3[k] = dim[k] - 1;
+            }
+            for (int z = lo3[2]; z <= hi3[2]; ++z)
+                for (int y = lo3[1]; y <= hi3[1]; ++y)
+                    for (int x = lo3[0]; x <= hi3[0]; ++x) {
+                        const int64_t c = x + (int64_t)dim[0] * (y + (int64_t)dim[1] * z);
+                        if (pass == 0) off[c + 1]++;
+                        else list[fill[c]++] = (int32_t)f;
+                    }
+        }
+        if (pass == 1) {
+            free(fill);
+            const double thr2 = threshold * threshold;
+#pragma omp parallel for schedule(dynamic, 65536)
+            for (int64_t i = 0; i < N; ++i) {
+                double q[3] = {0.0, 0.0, 0.0};
+                int bad = 0;
+                for (int k = 0; k < 4; ++k) {
+                    const int32_t vi = tets[i * 4 + k];
+                    if (vi < 0 || vi >= nv) { bad = 1; break; }
+                    q[0] += V[(size_t)vi * 3];
+                    q[1] += V[(size_t)vi * 3 + 1];
+                    q[2] += V[(size_t)vi * 3 + 2];
+                }
+                uint8_t lab = 1;
+                if (!bad) {
+                    int g[3], inside = 1;
+                    for (int k = 0; k < 3; ++k) {
+                        q[k] = (q[k] * 0.25) * cs[k] + co[k];
+                        const double t = (q[k] - bmin[k]) * inv[k];
+                        if (t < 0.0 || t >= (double)dim[k]) { inside = 0; break; }
+                        g[k] = (int)t;
+                    }
+                    if (inside) {
+                        const int64_t c = g[0] + (int64_t)dim[0] * (g[1] + (int64_t)dim[1] * g[2]);
+                        for (int64_t e = off[c]; e < off[c + 1]; ++e) {
+                            const int32_t f = list[e];
+                            if (pt_tri_d2(q, MV + (size_t)TF[f * 3] * 3, MV + (size_t)TF[f * 3 + 1] * 3,
+                                          MV + (size_t)TF[f * 3 + 2] * 3) <= thr2) { lab = 0; break; }
+                        }
+                    }
+                }
+                labels[i] = lab;
+            }
+            free(list);
+        }
+    }
+    free(off);
+    free(MV);
+    return 0;
+}
