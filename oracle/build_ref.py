@@ -44,6 +44,13 @@ def build(src: Path = DEFAULT_SRC, quiet: bool = False, force: bool = False) -> 
     bdir = OUT / "build"
     bdir.mkdir(exist_ok=True)
     os.environ.setdefault("MAX_JOBS", "4")
+    # The system toolchain: a compiler wrapper that links the C++ runtime
+    # statically into the module leaves two libstdc++ copies in the process,
+    # which crashes the reference on its first std::cout of a double.
+    for var, tool in (("CC", "gcc"), ("CXX", "g++")):
+        path = shutil.which(tool, path="/usr/bin") or shutil.which(tool)
+        if path:
+            os.environ[var] = path
     from torch.utils.cpp_extension import load
 
     mod = load(

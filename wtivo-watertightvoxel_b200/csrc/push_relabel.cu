@@ -56,6 +56,19 @@ __device__ __forceinline__ T warp_block_sum(T v, T* sh)
     return t;
 }
 
+// Copy a block's staged entries to a global queue of capacity cap.  Queue
+// entries are unique by construction (each node is appended at most once per
+// round or BFS); the guard keeps the writes inside the buffer even if that
+// invariant were broken, and reports it instead.
+__device__ __forceinline__ void flush_stage(const uint32_t* s_src, uint32_t count, uint32_t base,
+                                            uint32_t* dst, uint32_t cap, Ctl* ctl)
+{
+    if (threadIdx.x == 0 && (uint64_t)base + count > cap)
+        atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_INVARIANT);
+    for (uint32_t j = threadIdx.x; j < count; j += DTPB)
+        if (base + j < cap) dst[base + j] = s_src[j];
+}
+
 __global__ void __launch_bounds__(DTPB) k_init_excess(uint32_t n, const int32_t* __restrict__ term,
                                                       long long* __restrict__ excess)
 {
@@ -91,8 +104,8 @@ __global__ void __launch_bounds__(DTPB) k_bfs_seed(SolveView g)
             s_ab = s_an ? atomicAdd(&ctl->act_cnt[0], s_an) : 0u;
         }
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < s_fn; j += DTPB) g.fr[1][s_fb + j] = s_fr[j];
-        for (uint32_t j = threadIdx.x; j < s_an; j += DTPB) g.act[0][s_ab + j] = s_act[j];
+        flush_stage(s_fr, s_fn, s_fb, g.fr[1], g.n, ctl);
+        flush_stage(s_act, s_an, s_ab, g.act[0], g.n, ctl);
         __syncthreads();
     }
 }
@@ -105,7 +118,7 @@ __global__ void __launch_bounds__(DTPB) k_bfs_level(SolveView g, uint32_t L)
     __shared__ uint32_t s_fc, s_ac, s_fn, s_an, s_fb, s_ab;
     __shared__ unsigned long long s_red[DTPB / 32];
     Ctl* ctl = g.ctl;
-    const uint32_t cnt = ldcg(&ctl->bfs_cnt[L % 3]);
+    const uint32_t cnt = min(ldcg(&ctl->bfs_cnt[L % 3]), g.n);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl->bfs_cnt[(L + 2) % 3] = 0u;
         if (cnt == 0) ctl->bfs_done = 1u;
@@ -147,8 +160,8 @@ __global__ void __launch_bounds__(DTPB) k_bfs_level(SolveView g, uint32_t L)
             s_ab = s_an ? atomicAdd(&ctl->act_cnt[0], s_an) : 0u;
         }
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < s_fn; j += DTPB) out[s_fb + j] = s_fr[j];
-        for (uint32_t j = threadIdx.x; j < s_an; j += DTPB) g.act[0][s_ab + j] = s_act[j];
+        flush_stage(s_fr, s_fn, s_fb, out, g.n, ctl);
+        flush_stage(s_act, s_an, s_ab, g.act[0], g.n, ctl);
         __syncthreads();
     }
     const unsigned long long vs = warp_block_sum(visits, s_red);
@@ -249,7 +262,7 @@ __global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
     __shared__ uint32_t s_cnt, s_n, s_base;
     __shared__ unsigned long long s_red[DTPB / 32];
     Ctl* ctl = g.ctl;
-    const uint32_t cnt = ldcg(&ctl->act_cnt[round % 3]);
+    const uint32_t cnt = min(ldcg(&ctl->act_cnt[round % 3]), g.n);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl->act_cnt[(round + 2) % 3] = 0u;
         if (cnt) atomicAdd(&ctl->rounds_done, 1u);
@@ -275,7 +288,7 @@ __global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
             s_base = s_n ? atomicAdd(gcnt, s_n) : 0u;
         }
         __syncthreads();
-        for (uint32_t j = threadIdx.x; j < s_n; j += DTPB) out[s_base + j] = s_buf[j];
+        flush_stage(s_buf, s_n, s_base, out, g.n, ctl);
         __syncthreads();
     }
     unsigned long long x;
