@@ -199,6 +199,35 @@ gpupr_status gpupr_surface_count(const uint8_t* labels, int labels_on_device,
 gpupr_status gpupr_surface_fetch(int32_t* faces, double* vertices_out,
                                  int out_on_device, void* stream);
 
+/*
+ * Allocation-free variant of gpupr_solve_reduced.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory during the call:
+ * an application whose own allocator already owns the device heap, or code
+ * that must not enter the CUDA allocator mid-pipeline.  Nothing is allocated
+ * on the device or the host on success: the solver's scratch (reverse slots,
+ * excess, heights, queues, control block; about 25 MiB) is a static device
+ * array inside this library, which every GPU that loads the library holds
+ * until the process exits.
+ *   n            at most 1,048,576 nodes; larger graphs are rejected with
+ *                GPUPR_ERR_INVALID_ARGUMENT
+ *   d_neighbors  int32[4n], d_residual uint32[4n], d_terminal int32[n]: the
+ *                reduced graph on the device, updated in place as in
+ *                gpupr_solve_reduced
+ *   d_partition  uint8[n] device output, 1 = the node reaches the sink
+ * The first call on a device looks up the array's device address (with that
+ * device current) and caches it; make that first call before any stream
+ * capture.  All calls share the one array and it keeps the last call's
+ * contents (the call clears what must start at zero): calls whose work
+ * overlaps on the GPU, from other streams or threads, race and corrupt each
+ * other, so serialise them.
+ */
+gpupr_status gpupr_solve_reduced_noalloc(uint32_t n, int32_t* d_neighbors,
+                                         uint32_t* d_residual, int32_t* d_terminal,
+                                         uint8_t* d_partition,
+                                         int32_t global_relabel_period,
+                                         uint64_t max_rounds, int32_t local_steps,
+                                         void* stream, gpupr_cut_stats* stats);
+
 /* Release device memory cached between calls (pool + scratch). */
 gpupr_status gpupr_release_cached_memory(void);
 

@@ -490,6 +490,40 @@ gpupr_status gpupr_surface_fetch(int32_t* faces, double* vertices_out, int out_o
     return guarded([&] { surface_fetch(faces, vertices_out, out_on_device, static_cast<cudaStream_t>(stream)); });
 }
 
+gpupr_status gpupr_solve_reduced_noalloc(uint32_t n, int32_t* d_neighbors, uint32_t* d_residual,
+                                         int32_t* d_terminal, uint8_t* d_partition,
+                                         int32_t global_relabel_period, uint64_t max_rounds,
+                                         int32_t local_steps, void* stream, gpupr_cut_stats* stats)
+{
+    return guarded([&] {
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        if (!n) return;
+        if (!d_neighbors || !d_residual || !d_terminal || !d_partition)
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "GPUPr-FAST-v6.30 null graph pointer"};
+        if (!aligned(d_neighbors, 16) || !aligned(d_residual, 16))
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "graph rows must be 16-byte aligned"};
+        select_device_for(d_neighbors, "graph");
+        const SolveOptions opt = resolve_options(nullptr, local_steps, global_relabel_period, max_rounds);
+        SolveResult sr;
+        solve_reduced_noalloc(n, d_neighbors, d_residual, d_terminal, d_partition, opt, s, sr);
+        if (stats) {
+            stats->raw_flow = sr.raw_flow;
+            stats->adjusted_flow = sr.raw_flow;
+            stats->rounds = sr.rounds;
+            stats->global_relabels = sr.relabels;
+            stats->local_steps = local_steps;
+            stats->solve_seconds = sr.solve_s;
+            stats->free_n = n;
+            stats->node_visits = sr.node_visits;
+            stats->pushes = sr.pushes;
+            stats->bfs_visits = sr.bfs_visits;
+            stats->bfs_levels = sr.bfs_levels;
+            stats->kernel_launches = sr.launches;
+        }
+    });
+}
+
 gpupr_status gpupr_release_cached_memory(void)
 {
     return guarded([&] {

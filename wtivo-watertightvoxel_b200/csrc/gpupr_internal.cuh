@@ -208,6 +208,15 @@ void surface_count(const uint8_t* labels, int l_dev, const double* vertices, uin
                    uint64_t* n_used, cudaStream_t s);
 void surface_fetch(int32_t* faces, double* verts, int out_dev, cudaStream_t s);
 
+// Allocation-free solve (push_relabel.cu): all scratch in a static device
+// array sized for NOALLOC_MAX_NODES nodes; the partition goes to d_partition.
+constexpr uint32_t NOALLOC_MAX_NODES = 1u << 20;
+void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t* d_term,
+                           uint8_t* d_partition, const SolveOptions& opt, cudaStream_t s,
+                           SolveResult& out);
+void compute_reverse_slots_noalloc(uint32_t n, const int4* d_nbr, uint8_t* d_rev, int32_t* d_err,
+                                   cudaStream_t s);
+
 // Bounded wait self test kernel driver.
 gpupr_status bounded_wait_selftest(uint32_t limit_us, cudaStream_t s);
 

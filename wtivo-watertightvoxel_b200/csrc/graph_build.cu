@@ -455,3 +455,24 @@ void partition_from_height(uint32_t n, const uint32_t* d_height, uint8_t* d_part
 }
 
 }  // namespace gpupr
+
+namespace gpupr {
+
+// Reverse slots with a caller-provided device error flag (no allocation);
+// used by the allocation-free solve.
+void compute_reverse_slots_noalloc(uint32_t n, const int4* d_nbr, uint8_t* d_rev, int32_t* d_err,
+                                   cudaStream_t s)
+{
+    GPUPR_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int32_t), s));
+    k_reverse_slots<<<grid_for(n), TPB, 0, s>>>(n, d_nbr, d_rev, d_err);
+    GPUPR_CUDA(cudaGetLastError());
+    int32_t e = 0;
+    GPUPR_CUDA(cudaMemcpyAsync(&e, d_err, sizeof(e), cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    if (e == GPUPR_ERR_NO_REVERSE)
+        throw Error{GPUPR_ERR_NO_REVERSE,
+                    "GPUPr-B200 device invariant failed: neighbor lists are not symmetric"};
+    if (e) throw Error{GPUPR_ERR_INVARIANT, "GPUPr-B200 device invariant failed: neighbor id >= n"};
+}
+
+}  // namespace gpupr

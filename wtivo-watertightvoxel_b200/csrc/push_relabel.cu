@@ -25,6 +25,7 @@
 #include <stdint.h>
 
 #include <chrono>
+#include <mutex>
 #include <cmath>
 #include <string>
 
@@ -579,6 +580,172 @@ gpupr_status bounded_wait_selftest(uint32_t limit_us, cudaStream_t s)
     GPUPR_CUDA(cudaMemcpyAsync(&h, st.p, sizeof(h), cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaStreamSynchronize(s));
     return (gpupr_status)h;
+}
+
+}  // namespace gpupr
+
+namespace gpupr {
+
+// ---------------------------------------------------------------------------
+// Allocation-free solve: scratch in a static device array.
+//
+// For callers that cannot allocate device memory (a host application that owns
+// the whole device heap through its own allocator, or a caller that must not
+// call the CUDA allocator mid-pipeline): every buffer the solver needs beyond
+// the caller's graph and output lives in g_noalloc_scratch below.  The array is
+// part of every context that loads this library, for the lifetime of the
+// process.  It is shared by all calls: two calls whose work overlaps on the GPU
+// (different streams or threads at the same time) corrupt each other.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t NA_ALIGN = 256;
+constexpr size_t na_round(size_t b) { return (b + NA_ALIGN - 1) / NA_ALIGN * NA_ALIGN; }
+// layout: control block | error flag | excess | height | 3 queues | reverse slots
+constexpr size_t NA_CTL = 0;
+constexpr size_t NA_ERR = na_round(sizeof(Ctl));
+constexpr size_t NA_EXCESS = NA_ERR + NA_ALIGN;
+constexpr size_t NA_HEIGHT = NA_EXCESS + na_round((size_t)NOALLOC_MAX_NODES * 8u);
+constexpr size_t NA_Q0 = NA_HEIGHT + na_round((size_t)NOALLOC_MAX_NODES * 4u);
+constexpr size_t NA_Q1 = NA_Q0 + na_round((size_t)NOALLOC_MAX_NODES * 4u);
+constexpr size_t NA_Q2 = NA_Q1 + na_round((size_t)NOALLOC_MAX_NODES * 4u);
+constexpr size_t NA_REV = NA_Q2 + na_round((size_t)NOALLOC_MAX_NODES * 4u);
+constexpr size_t NA_BYTES = NA_REV + na_round((size_t)NOALLOC_MAX_NODES);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+std::mutex g_na_mu;
+unsigned char* g_na_ptr[64] = {};
+
+// Device address of the scratch array on the current device.  The host-side
+// name g_noalloc_scratch is only a stand-in for the symbol, so the address is
+// looked up once per device (with that device current) and cached.
+unsigned char* noalloc_scratch()
+{
+    int dev = 0;
+    GPUPR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "device ordinal out of range"};
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    if (!g_na_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            throw Error{GPUPR_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch) failed: ") +
+                                            cudaGetErrorString(e)};
+        g_na_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    return g_na_ptr[dev];
+}
+
+// Host copy of the control block without pinned memory: a pageable
+// cudaMemcpyAsync on the stream, then a stream synchronize.
+const Ctl& read_ctl_stack(Ctl& h, const Ctl* d, cudaStream_t s)
+{
+    GPUPR_CUDA(cudaMemcpyAsync(&h, d, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    if (h.error)
+        throw Error{(gpupr_status)h.error, "GPUPr-B200 device invariant failed"};
+    return h;
+}
+
+}  // namespace
+
+void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t* d_term,
+                           uint8_t* d_partition, const SolveOptions& opt, cudaStream_t s,
+                           SolveResult& out)
+{
+    using Clock = std::chrono::steady_clock;
+    out = SolveResult{};
+    if (!n) return;
+    if (n > NOALLOC_MAX_NODES)
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT,
+                    "gpupr_solve_reduced_noalloc: n exceeds the static scratch limit of 1048576 nodes"};
+    unsigned char* base = noalloc_scratch();
+    Ctl* ctl = reinterpret_cast<Ctl*>(base + NA_CTL);
+    int32_t* err = reinterpret_cast<int32_t*>(base + NA_ERR);
+    uint8_t* rev = base + NA_REV;
+    const int4* nbr = reinterpret_cast<const int4*>(d_nbr);
+    compute_reverse_slots_noalloc(n, nbr, rev, err, s);
+    out.launches += 1;
+
+    SolveView g{};
+    g.n = n;
+    g.nbr = nbr;
+    g.res = d_res;
+    g.rev = rev;
+    g.term = d_term;
+    g.excess = reinterpret_cast<long long*>(base + NA_EXCESS);
+    g.height = reinterpret_cast<uint32_t*>(base + NA_HEIGHT);
+    g.act[0] = reinterpret_cast<uint32_t*>(base + NA_Q0);
+    g.act[1] = reinterpret_cast<uint32_t*>(base + NA_Q1);
+    g.fr[0] = reinterpret_cast<uint32_t*>(base + NA_Q2);
+    g.fr[1] = g.act[1];
+    g.ctl = ctl;
+    g.local_steps = opt.local_steps;
+    const int grid = sm_count() * (opt.blocks_per_sm > 0 ? opt.blocks_per_sm : 4);
+
+    Ctl hc{};
+    // the array keeps the previous call's contents: the control block must
+    // start at zero; every other buffer is written before it is read
+    GPUPR_CUDA(cudaMemsetAsync(ctl, 0, sizeof(Ctl), s));
+    k_init_excess<<<grid, DTPB, 0, s>>>(n, d_term, g.excess);
+    GPUPR_CUDA(cudaGetLastError());
+    out.launches += 1;
+    const auto t0 = Clock::now();
+    uint64_t rounds_total = 0;
+    for (;;) {
+        GPUPR_CUDA(cudaMemsetAsync(ctl, 0, offsetof(Ctl, error), s));
+        k_bfs_seed<<<grid, DTPB, 0, s>>>(g);
+        GPUPR_CUDA(cudaGetLastError());
+        out.launches += 1;
+        uint32_t L = 1;
+        for (;;) {
+            for (int b = 0; b < opt.bfs_batch; ++b, ++L) {
+                k_bfs_level<<<grid, DTPB, 0, s>>>(g, L);
+                GPUPR_CUDA(cudaGetLastError());
+            }
+            out.launches += (uint64_t)opt.bfs_batch;
+            read_ctl_stack(hc, ctl, s);
+            if (hc.bfs_done) break;
+            if ((uint64_t)L > (uint64_t)n + 2u)
+                throw Error{GPUPR_ERR_INVARIANT, "GPUPr-FAST-v6.30 BFS exceeded n+1 levels"};
+        }
+        ++out.relabels;
+        out.bfs_levels += hc.bfs_levels;
+        if (hc.act_cnt[0] == 0) break;
+        if (rounds_total >= opt.max_rounds)
+            throw Error{GPUPR_ERR_MAX_ROUNDS, "GPUPr-FAST-v6.30 max macro rounds exceeded"};
+        const unsigned long long visits0 = hc.node_visits;
+        uint32_t r = 0;
+        for (;;) {
+            const uint64_t left = opt.max_rounds - rounds_total;
+            int batch = opt.round_batch;
+            if ((uint64_t)batch > left) batch = (int)left;
+            for (int b = 0; b < batch; ++b, ++r) {
+                k_discharge<<<grid, DTPB, 0, s>>>(g, r);
+                GPUPR_CUDA(cudaGetLastError());
+            }
+            out.launches += (uint64_t)batch;
+            read_ctl_stack(hc, ctl, s);
+            rounds_total = hc.rounds_done;
+            if (hc.act_cnt[r % 3] == 0u) break;
+            if (rounds_total >= opt.max_rounds)
+                throw Error{GPUPR_ERR_MAX_ROUNDS, "GPUPr-FAST-v6.30 max macro rounds exceeded"};
+            if (opt.relabel_rounds > 0 && r >= (uint32_t)opt.relabel_rounds) break;
+            if (opt.work_factor > 0 && (double)(hc.node_visits - visits0) > opt.work_factor * (double)n)
+                break;
+            if (std::chrono::duration<double>(Clock::now() - t0).count() > opt.time_limit_s)
+                throw Error{GPUPR_ERR_TIMEOUT, "GPUPr-FAST-v6.30 solve exceeded 240s safety limit"};
+        }
+    }
+    partition_from_height(n, g.height, d_partition, s, &out.launches);
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    out.raw_flow = (int64_t)hc.sink_flow;
+    out.rounds = hc.rounds_done;
+    out.node_visits = hc.node_visits;
+    out.pushes = hc.pushes;
+    out.bfs_visits = hc.bfs_visits;
+    out.solve_s = std::chrono::duration<double>(Clock::now() - t0).count();
 }
 
 }  // namespace gpupr

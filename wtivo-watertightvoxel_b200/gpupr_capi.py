@@ -101,6 +101,7 @@ def lib():
         L.gpupr_solve_ell.argtypes = [ctypes.c_uint32, p, p, p, p, p, p, p, p, p]
         L.gpupr_surface_count.argtypes = [p, ctypes.c_int, p, u64, ctypes.c_int, p, p, u64, p, p, p]
         L.gpupr_surface_fetch.argtypes = [p, p, ctypes.c_int, p]
+        L.gpupr_solve_reduced_noalloc.argtypes = [ctypes.c_uint32, p, p, p, p, i32, u64, i32, p, p]
         L.gpupr_release_cached_memory.argtypes = []
         L.gpupr_selftest_bounded_wait.argtypes = [ctypes.c_uint32, p]
         for name in header_functions():
