@@ -75,6 +75,7 @@ typedef struct {
     double bfs_ms;              /* CUDA-event time of all global-relabel BFS */
     uint64_t discharge_launches;
     uint64_t bfs_launches;
+    int64_t engine;             /* 1 one launch per step, 2 persistent */
 } gpupr_cut_stats;
 
 /* Solver tuning knobs; zero fields take the defaults shown. */
@@ -89,6 +90,9 @@ typedef struct {
     int32_t blocks_per_sm;        /* persistent grid multiplier, default 4 */
     double work_relabel_factor;   /* relabel after this many node visits per
                                      free node since the last one (default 3) */
+    int32_t engine;               /* 0 auto (persistent when the device supports
+                                     cooperative launch), 1 one launch per BFS
+                                     level / round, 2 persistent */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

@@ -93,7 +93,9 @@ def test_solver_invariants(built, kind, seed, size):
 @pytest.mark.parametrize("opt", [dict(local_steps=1), dict(local_steps=32),
                                  dict(global_relabel_period=0), dict(global_relabel_period=16),
                                  dict(blocks_per_sm=1, round_batch=3, bfs_batch=2),
-                                 dict(work_relabel_factor=0.05)])
+                                 dict(work_relabel_factor=0.05), dict(engine=1), dict(engine=2),
+                                 dict(engine=2, blocks_per_sm=1), dict(engine=2, local_steps=1),
+                                 dict(engine=2, global_relabel_period=-1, work_relabel_factor=0.1)])
 def test_options_do_not_change_the_cut(built, opt):
     import gpupr_capi
 

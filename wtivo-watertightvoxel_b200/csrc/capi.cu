@@ -216,6 +216,7 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
     st->bfs_ms = sr.bfs_ms;
     st->discharge_launches = sr.discharge_launches;
     st->bfs_launches = sr.bfs_launches;
+    st->engine = sr.engine;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -404,6 +405,7 @@ gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_r
             stats->bfs_ms = sr.bfs_ms;
             stats->discharge_launches = sr.discharge_launches;
             stats->bfs_launches = sr.bfs_launches;
+            stats->engine = sr.engine;
             stats->kernel_launches = launches;
         }
     });
@@ -459,6 +461,7 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
             stats->bfs_ms = sr.bfs_ms;
             stats->discharge_launches = sr.discharge_launches;
             stats->bfs_launches = sr.bfs_launches;
+            stats->engine = sr.engine;
             stats->kernel_launches = launches;
         }
     });

@@ -33,7 +33,11 @@ struct Ctl {
     unsigned long long pushes;
     unsigned long long bfs_visits;
     unsigned long long relabels;
-    unsigned long long reserved[4];
+    uint32_t bar_arrive;     // persistent engine: grid barrier arrivals
+    uint32_t bar_gen;        // persistent engine: grid barrier generation
+    uint32_t relabel_phases; // persistent engine: global relabels run
+    uint32_t pad0;
+    unsigned long long reserved[2];
 };
 
 // View of the reduced graph + solver workspace handed to kernels.
@@ -168,6 +172,7 @@ struct SolveOptions {
     int block = 256;
     int blocks_per_sm = 4;
     double work_factor = 3.0;
+    int engine = 0;                // 0 auto, 1 one launch per step, 2 persistent
 };
 
 SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw,
@@ -192,6 +197,7 @@ struct SolveResult {
     double discharge_ms = 0.0, bfs_ms = 0.0;
     uint64_t discharge_launches = 0, bfs_launches = 0;
     uint64_t workspace_bytes = 0;
+    int engine = 1;                // 1 one launch per step, 2 persistent
 };
 
 // Phase-I push-relabel on a reduced graph (res/term updated in place).

@@ -80,63 +80,52 @@ __global__ void __launch_bounds__(DTPB) k_init_excess(uint32_t n, const int32_t*
 }
 
 // Level 1 of the backward BFS: nodes with a residual arc to the sink.  Every
-// other height is reset to UNVIS (.cu:374-379).
-__global__ void __launch_bounds__(DTPB) k_bfs_seed(SolveView g)
+// other height is reset to UNVIS (.cu:374-379).  s_m[0..5] are the block's
+// staging counters (frontier count, active count, and their flush copies).
+__device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr, uint32_t* s_act,
+                                              uint32_t* s_m)
 {
-    __shared__ uint32_t s_fr[DTPB], s_act[DTPB];
-    __shared__ uint32_t s_fc, s_ac, s_fn, s_an, s_fb, s_ab;
     Ctl* ctl = g.ctl;
-    if (threadIdx.x == 0) { s_fc = 0; s_ac = 0; }
-    __syncthreads();
     for (uint32_t base = blockIdx.x * DTPB; base < g.n; base += gridDim.x * DTPB) {
         const uint32_t v = base + threadIdx.x;
         if (v < g.n) {
             const int32_t t = ldcg(g.term + v);
             g.height[v] = (t < 0) ? 1u : UNVIS;
             if (t < 0) {
-                s_fr[atomicAdd(&s_fc, 1u)] = v;
-                if (1u < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_ac, 1u)] = v;
+                s_fr[atomicAdd(&s_m[0], 1u)] = v;
+                if (1u < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_m[1], 1u)] = v;
             }
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            s_fn = s_fc; s_an = s_ac; s_fc = 0; s_ac = 0;
-            s_fb = s_fn ? atomicAdd(&ctl->bfs_cnt[1], s_fn) : 0u;
-            s_ab = s_an ? atomicAdd(&ctl->act_cnt[0], s_an) : 0u;
+            s_m[2] = s_m[0]; s_m[3] = s_m[1]; s_m[0] = 0; s_m[1] = 0;
+            s_m[4] = s_m[2] ? atomicAdd(&ctl->bfs_cnt[1], s_m[2]) : 0u;
+            s_m[5] = s_m[3] ? atomicAdd(&ctl->act_cnt[0], s_m[3]) : 0u;
         }
         __syncthreads();
-        flush_stage(s_fr, s_fn, s_fb, g.fr[1], g.n, ctl);
-        flush_stage(s_act, s_an, s_ab, g.act[0], g.n, ctl);
+        flush_stage(s_fr, s_m[2], s_m[4], g.fr[1], g.n, ctl);
+        flush_stage(s_act, s_m[3], s_m[5], g.act[0], g.n, ctl);
         __syncthreads();
     }
 }
 
-// One top-down BFS level L: frontier nodes u (height L) label every
-// unvisited neighbor v with a residual arc v->u as L+1 (.cu:103-139).
-__global__ void __launch_bounds__(DTPB) k_bfs_level(SolveView g, uint32_t L)
+// One top-down BFS level L over cnt frontier nodes: each frontier node u
+// (height L) labels every unvisited neighbor v with a residual arc v->u as
+// L+1 (.cu:103-139) and appends it to the next frontier, and to the active
+// queue when it holds excess.
+__device__ __forceinline__ void bfs_level_body(const SolveView& g, uint32_t L, uint32_t cnt,
+                                               uint32_t* s_fr, uint32_t* s_act, uint32_t* s_m,
+                                               unsigned long long& visits)
 {
-    __shared__ uint32_t s_fr[DTPB * 4], s_act[DTPB * 4];
-    __shared__ uint32_t s_fc, s_ac, s_fn, s_an, s_fb, s_ab;
-    __shared__ unsigned long long s_red[DTPB / 32];
     Ctl* ctl = g.ctl;
-    const uint32_t cnt = min(ldcg(&ctl->bfs_cnt[L % 3]), g.n);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->bfs_cnt[(L + 2) % 3] = 0u;
-        if (cnt == 0) ctl->bfs_done = 1u;
-        else atomicAdd(&ctl->bfs_levels, 1u);
-    }
-    if (cnt == 0) return;
     const uint32_t* in = (L & 1) ? g.fr[1] : g.fr[0];
     uint32_t* out = (L & 1) ? g.fr[0] : g.fr[1];
     uint32_t* gcnt = &ctl->bfs_cnt[(L + 1) % 3];
     const uint32_t newh = L + 1u;
-    unsigned long long visits = 0;
-    if (threadIdx.x == 0) { s_fc = 0; s_ac = 0; }
-    __syncthreads();
     for (uint32_t base = blockIdx.x * DTPB; base < cnt; base += gridDim.x * DTPB) {
         const uint32_t i = base + threadIdx.x;
         if (i < cnt) {
-            const uint32_t u = __ldg(in + i);
+            const uint32_t u = __ldcg(in + i);
             const int4 nb4 = __ldg(g.nbr + u);
             const uint32_t rv = __ldg(g.rev + u);
             const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
@@ -149,22 +138,50 @@ __global__ void __launch_bounds__(DTPB) k_bfs_level(SolveView g, uint32_t L)
                 const uint32_t rk = (rv >> (2 * k)) & 3u;
                 if (ldcg(g.res + (size_t)v * 4u + rk) == 0u) continue;
                 if (atomicCAS(g.height + v, UNVIS, newh) == UNVIS) {
-                    s_fr[atomicAdd(&s_fc, 1u)] = (uint32_t)v;
-                    if (newh < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_ac, 1u)] = (uint32_t)v;
+                    s_fr[atomicAdd(&s_m[0], 1u)] = (uint32_t)v;
+                    if (newh < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_m[1], 1u)] = (uint32_t)v;
                 }
             }
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            s_fn = s_fc; s_an = s_ac; s_fc = 0; s_ac = 0;
-            s_fb = s_fn ? atomicAdd(gcnt, s_fn) : 0u;
-            s_ab = s_an ? atomicAdd(&ctl->act_cnt[0], s_an) : 0u;
+            s_m[2] = s_m[0]; s_m[3] = s_m[1]; s_m[0] = 0; s_m[1] = 0;
+            s_m[4] = s_m[2] ? atomicAdd(gcnt, s_m[2]) : 0u;
+            s_m[5] = s_m[3] ? atomicAdd(&ctl->act_cnt[0], s_m[3]) : 0u;
         }
         __syncthreads();
-        flush_stage(s_fr, s_fn, s_fb, out, g.n, ctl);
-        flush_stage(s_act, s_an, s_ab, g.act[0], g.n, ctl);
+        flush_stage(s_fr, s_m[2], s_m[4], out, g.n, ctl);
+        flush_stage(s_act, s_m[3], s_m[5], g.act[0], g.n, ctl);
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(DTPB) k_bfs_seed(SolveView g)
+{
+    __shared__ uint32_t s_fr[DTPB], s_act[DTPB];
+    __shared__ uint32_t s_m[8];
+    if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
+    __syncthreads();
+    bfs_seed_body(g, s_fr, s_act, s_m);
+}
+
+__global__ void __launch_bounds__(DTPB) k_bfs_level(SolveView g, uint32_t L)
+{
+    __shared__ uint32_t s_fr[DTPB * 4], s_act[DTPB * 4];
+    __shared__ uint32_t s_m[8];
+    __shared__ unsigned long long s_red[DTPB / 32];
+    Ctl* ctl = g.ctl;
+    const uint32_t cnt = min(ldcg(&ctl->bfs_cnt[L % 3]), g.n);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->bfs_cnt[(L + 2) % 3] = 0u;
+        if (cnt == 0) ctl->bfs_done = 1u;
+        else atomicAdd(&ctl->bfs_levels, 1u);
+    }
+    if (cnt == 0) return;
+    unsigned long long visits = 0;
+    if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
+    __syncthreads();
+    bfs_level_body(g, L, cnt, s_fr, s_act, s_m, visits);
     const unsigned long long vs = warp_block_sum(visits, s_red);
     if (threadIdx.x == 0 && vs) atomicAdd(&ctl->bfs_visits, vs);
 }
@@ -183,14 +200,14 @@ __device__ __forceinline__ void discharge_node(const SolveView& g, uint32_t v, u
                                                uint32_t* s_cnt, Work& w)
 {
     const uint32_t n = g.n;
-    uint32_t h = g.height[v];
+    uint32_t h = ldcg(g.height + v);   // L2: a previous owner may have run on another SM
     if (h >= n) return;
     long long ex = ldcg(g.excess + v);
     if (ex <= 0) return;
     const int4 nb4 = __ldg(g.nbr + v);
     const uint4 r4 = __ldcg(reinterpret_cast<const uint4*>(g.res) + v);
     const uint32_t rv = __ldg(g.rev + v);
-    int32_t t = g.term[v];
+    int32_t t = ldcg(g.term + v);
     const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
     uint32_t r[4] = {r4.x, r4.y, r4.z, r4.w};
     uint32_t hn[4];
@@ -257,41 +274,37 @@ __device__ __forceinline__ void discharge_node(const SolveView& g, uint32_t v, u
     if (now > 0 && h < n) s_buf[atomicAdd(s_cnt, 1u)] = v;   // keeps ownership
 }
 
-__global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
+// One discharge round over cnt active nodes: discharge each, stage the nodes
+// that become (or stay) active, append them to the next active queue.
+__device__ __forceinline__ void discharge_body(const SolveView& g, uint32_t round, uint32_t cnt,
+                                               uint32_t* s_buf, uint32_t* s_m, Work& w)
 {
-    __shared__ uint32_t s_buf[DTPB * 5];
-    __shared__ uint32_t s_cnt, s_n, s_base;
-    __shared__ unsigned long long s_red[DTPB / 32];
     Ctl* ctl = g.ctl;
-    const uint32_t cnt = min(ldcg(&ctl->act_cnt[round % 3]), g.n);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->act_cnt[(round + 2) % 3] = 0u;
-        if (cnt) atomicAdd(&ctl->rounds_done, 1u);
-    }
-    if (cnt == 0) return;
     const uint32_t* in = (round & 1) ? g.act[1] : g.act[0];
     uint32_t* out = (round & 1) ? g.act[0] : g.act[1];
     uint32_t* gcnt = &ctl->act_cnt[(round + 1) % 3];
-    Work w;
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
     for (uint32_t base = blockIdx.x * DTPB; base < cnt; base += gridDim.x * DTPB) {
         const uint32_t i = base + threadIdx.x;
         if (i < cnt) {
-            const uint32_t v = __ldg(in + i);
-            if (v < g.n) discharge_node(g, v, s_buf, &s_cnt, w);
+            const uint32_t v = __ldcg(in + i);
+            if (v < g.n) discharge_node(g, v, s_buf, &s_m[0], w);
             else atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_INVARIANT);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            s_n = s_cnt;
-            s_cnt = 0;
-            s_base = s_n ? atomicAdd(gcnt, s_n) : 0u;
+            s_m[2] = s_m[0];
+            s_m[0] = 0;
+            s_m[4] = s_m[2] ? atomicAdd(gcnt, s_m[2]) : 0u;
         }
         __syncthreads();
-        flush_stage(s_buf, s_n, s_base, out, g.n, ctl);
+        flush_stage(s_buf, s_m[2], s_m[4], out, g.n, ctl);
         __syncthreads();
     }
+}
+
+__device__ __forceinline__ void reduce_work(Ctl* ctl, const Work& w, unsigned long long bfs_visits,
+                                            unsigned long long* s_red)
+{
     unsigned long long x;
     x = warp_block_sum(w.visits, s_red);
     if (threadIdx.x == 0 && x) atomicAdd(&ctl->node_visits, x);
@@ -301,6 +314,160 @@ __global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
     if (threadIdx.x == 0 && x) atomicAdd(&ctl->relabels, x);
     x = warp_block_sum(w.sink, s_red);
     if (threadIdx.x == 0 && x) atomicAdd(&ctl->sink_flow, x);
+    x = warp_block_sum(bfs_visits, s_red);
+    if (threadIdx.x == 0 && x) atomicAdd(&ctl->bfs_visits, x);
+}
+
+__global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
+{
+    __shared__ uint32_t s_buf[DTPB * 5];
+    __shared__ uint32_t s_m[8];
+    __shared__ unsigned long long s_red[DTPB / 32];
+    Ctl* ctl = g.ctl;
+    const uint32_t cnt = min(ldcg(&ctl->act_cnt[round % 3]), g.n);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->act_cnt[(round + 2) % 3] = 0u;
+        if (cnt) atomicAdd(&ctl->rounds_done, 1u);
+    }
+    if (cnt == 0) return;
+    Work w;
+    if (threadIdx.x == 0) s_m[0] = 0;
+    __syncthreads();
+    discharge_body(g, round, cnt, s_buf, s_m, w);
+    reduce_work(ctl, w, 0ull, s_red);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent engine: the whole solve in one cooperative launch.  The same
+// level and round steps as above run back to back, separated by a software
+// grid barrier instead of a kernel boundary, and the control decisions
+// (frontier/queue empty, relabel period, work budget, round limit) are taken
+// by every block from the same counters read after a barrier, so all blocks
+// follow the same path.  Every barrier wait is bounded; an error or the time
+// limit makes every block leave at its next barrier.
+// ---------------------------------------------------------------------------
+struct PersistParams {
+    unsigned long long max_rounds;
+    unsigned long long budget;      // node visits per discharge phase, 0 = none
+    unsigned long long limit_ns;    // solve time limit
+    unsigned long long wait_ns;     // bound of one barrier wait
+    uint32_t relabel_rounds;        // rounds per discharge phase, 0 = none
+};
+
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <class T>
+__device__ __forceinline__ T vload(const T* p) { return *reinterpret_cast<const volatile T*>(p); }
+
+__device__ bool grid_barrier(Ctl* ctl, unsigned long long deadline, unsigned long long wait_ns,
+                             int* s_ok)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int gen = vload(&ctl->bar_gen);
+        __threadfence();
+        if (atomicAdd(&ctl->bar_arrive, 1u) == gridDim.x - 1) {
+            if (gtimer() > deadline) atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_TIMEOUT);
+            atomicExch(&ctl->bar_arrive, 0u);
+            __threadfence();
+            atomicAdd(&ctl->bar_gen, 1u);
+        } else {
+            const unsigned long long t0 = gtimer();
+            while (vload(&ctl->bar_gen) == gen) {
+                if (vload(&ctl->error)) break;
+                if (gtimer() - t0 > wait_ns) {
+                    atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_TIMEOUT);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        *s_ok = vload(&ctl->error) == 0;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+__global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistParams p)
+{
+    __shared__ uint32_t s_buf[DTPB * 8];
+    __shared__ uint32_t s_m[8];
+    __shared__ unsigned long long s_red[DTPB / 32];
+    __shared__ int s_ok;
+    Ctl* ctl = g.ctl;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    const unsigned long long deadline = gtimer() + p.limit_ns;
+    Work w;
+    unsigned long long bfs_visits = 0;
+    if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
+    for (uint32_t v = blockIdx.x * DTPB + threadIdx.x; v < g.n; v += gridDim.x * DTPB) {
+        const int32_t t = ldcg(g.term + v);
+        g.excess[v] = t > 0 ? (long long)t : 0ll;   // source arc saturated (.cu:69-83)
+    }
+    if (grid_barrier(ctl, deadline, p.wait_ns, &s_ok)) {
+        unsigned long long rounds_total = 0;
+        uint32_t levels_total = 0, relabels = 0;
+        bool ok = true;
+        while (ok) {
+            // ---- exact global relabel ----
+            bfs_seed_body(g, s_buf, s_buf + DTPB * 4, s_m);
+            if (!(ok = grid_barrier(ctl, deadline, p.wait_ns, &s_ok))) break;
+            uint32_t L = 1;
+            for (;;) {
+                const uint32_t cnt = min(vload(&ctl->bfs_cnt[L % 3]), g.n);
+                if (cnt == 0) break;
+                if (lead) ctl->bfs_cnt[(L + 2) % 3] = 0u;
+                bfs_level_body(g, L, cnt, s_buf, s_buf + DTPB * 4, s_m, bfs_visits);
+                if (!(ok = grid_barrier(ctl, deadline, p.wait_ns, &s_ok))) break;
+                ++L;
+                ++levels_total;
+                if (L > g.n + 2u) {   // a BFS labels a new node per level
+                    if (lead) atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_INVARIANT);
+                    ok = false;
+                    break;
+                }
+            }
+            if (!ok) break;
+            ++relabels;
+            if (vload(&ctl->act_cnt[0]) == 0u) break;   // maximum preflow
+            // ---- discharge rounds ----
+            uint32_t r = 0;
+            unsigned long long visits = 0;
+            for (;;) {
+                const uint32_t cnt = min(vload(&ctl->act_cnt[r % 3]), g.n);
+                if (cnt == 0) break;
+                if (rounds_total >= p.max_rounds) {
+                    if (lead) atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_MAX_ROUNDS);
+                    ok = false;
+                    break;
+                }
+                if (lead) ctl->act_cnt[(r + 2) % 3] = 0u;
+                discharge_body(g, r, cnt, s_buf, s_m, w);
+                if (!(ok = grid_barrier(ctl, deadline, p.wait_ns, &s_ok))) break;
+                ++r;
+                ++rounds_total;
+                visits += cnt;
+                if (p.relabel_rounds && r >= p.relabel_rounds) break;
+                if (p.budget && visits > p.budget) break;
+            }
+            if (!ok) break;
+            if (lead) {
+                for (int k = 0; k < 3; ++k) { ctl->act_cnt[k] = 0u; ctl->bfs_cnt[k] = 0u; }
+            }
+            if (!(ok = grid_barrier(ctl, deadline, p.wait_ns, &s_ok))) break;
+        }
+        if (lead) {
+            ctl->rounds_done = (uint32_t)rounds_total;
+            ctl->bfs_levels = levels_total;
+            ctl->relabel_phases = relabels;
+        }
+    }
+    reduce_work(ctl, w, bfs_visits, s_red);
 }
 
 __global__ void __launch_bounds__(DTPB) k_prepare_raw(uint32_t n, const int4* __restrict__ nbr,
@@ -395,6 +562,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
         if (o->block_size > 0) r.block = o->block_size;
         if (o->blocks_per_sm > 0) r.blocks_per_sm = o->blocks_per_sm;
         if (o->work_relabel_factor > 0) r.work_factor = o->work_relabel_factor;
+        r.engine = o->engine;
     }
     // clamps of gpu_push_relabel_fast.cu:421-424 and :476-480
     if (ls < 1) ls = 1;
@@ -405,6 +573,77 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
     r.relabel_rounds = period > 0 ? ((period + ls - 1) / ls < 1 ? 1 : (period + ls - 1) / ls) : 0;
     r.max_rounds = mr;
     return r;
+}
+
+bool use_persistent_engine(const SolveOptions& opt)
+{
+    if (opt.engine == 1) return false;
+    int dev = 0, coop = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return coop != 0;
+}
+
+// The whole solve as one cooperative launch of k_solve_persistent.
+void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t s, SolveResult& out)
+{
+    using Clock = std::chrono::steady_clock;
+    int bps = 0;
+    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent, DTPB, 0));
+    if (bps < 1) throw Error{GPUPR_ERR_CUDA, "persistent solver kernel cannot be resident"};
+    const int want = opt.blocks_per_sm > 0 ? opt.blocks_per_sm : 4;
+    const unsigned grid = (unsigned)(sm_count() * (want < bps ? want : bps));
+    PersistParams p{};
+    p.max_rounds = opt.max_rounds;
+    p.relabel_rounds = (uint32_t)(opt.relabel_rounds > 0 ? opt.relabel_rounds : 0);
+    const double budget = opt.work_factor > 0 ? opt.work_factor * (double)g.n : 0.0;
+    p.budget = budget > 1.8e19 ? 0ull : (unsigned long long)budget;
+    p.limit_ns = (unsigned long long)(opt.time_limit_s * 1e9);
+    p.wait_ns = 10ull * 1000ull * 1000ull * 1000ull;   // one step never takes this long
+
+    PinnedCtl pc;
+    cudaEvent_t e0, e1;
+    GPUPR_CUDA(cudaEventCreate(&e0));
+    GPUPR_CUDA(cudaEventCreate(&e1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } evg{e0, e1};
+    const auto t0 = Clock::now();
+    GPUPR_CUDA(cudaMemsetAsync(g.ctl, 0, sizeof(Ctl), s));
+    GPUPR_CUDA(cudaEventRecord(e0, s));
+    SolveView gv = g;
+    void* args[] = {&gv, &p};
+    GPUPR_CUDA(cudaLaunchCooperativeKernel((const void*)k_solve_persistent, dim3(grid), dim3(DTPB),
+                                           args, 0, s));
+    GPUPR_CUDA(cudaEventRecord(e1, s));
+    GPUPR_CUDA(cudaMemcpyAsync(pc.h, g.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    const Ctl& hc = *pc.h;
+    if (hc.error == (int)GPUPR_ERR_TIMEOUT)
+        throw Error{GPUPR_ERR_TIMEOUT, "GPUPr-FAST-v6.30 solve exceeded 240s safety limit"};
+    if (hc.error == (int)GPUPR_ERR_MAX_ROUNDS)
+        throw Error{GPUPR_ERR_MAX_ROUNDS, "GPUPr-FAST-v6.30 max macro rounds exceeded"};
+    if (hc.error)
+        throw Error{(gpupr_status)hc.error,
+                    "GPUPr-B200 device invariant failed code=" + std::to_string(hc.error)};
+    float ms = 0.f;
+    GPUPR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    out.engine = 2;
+    out.launches = 1;
+    out.raw_flow = (int64_t)hc.sink_flow;
+    out.rounds = hc.rounds_done;
+    out.relabels = hc.relabel_phases;
+    out.node_visits = hc.node_visits;
+    out.pushes = hc.pushes;
+    out.bfs_visits = hc.bfs_visits;
+    out.bfs_levels = hc.bfs_levels;
+    out.solve_device_ms = ms;
+    out.discharge_launches = 1;
+    out.solve_s = std::chrono::duration<double>(Clock::now() - t0).count();
 }
 
 void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const uint8_t* d_rev,
@@ -439,6 +678,11 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
     g.ctl = w.ctl.p;
     g.local_steps = opt.local_steps;
 
+    if (use_persistent_engine(opt)) {
+        solve_persistent(g, opt, s, out);
+        return;
+    }
+    out.engine = 1;
     const int grid = sm_count() * (opt.blocks_per_sm > 0 ? opt.blocks_per_sm : 4);
     PinnedCtl pc;
     cudaEvent_t e0, e1, ba, bb;

@@ -34,7 +34,7 @@ STATS_FIELDS = [
     ("kernel_launches", ctypes.c_uint64), ("solve_device_ms", ctypes.c_double),
     ("build_device_ms", ctypes.c_double), ("discharge_ms", ctypes.c_double),
     ("bfs_ms", ctypes.c_double), ("discharge_launches", ctypes.c_uint64),
-    ("bfs_launches", ctypes.c_uint64),
+    ("bfs_launches", ctypes.c_uint64), ("engine", ctypes.c_int64),
 ]
 
 
@@ -51,7 +51,7 @@ class SolveOptions(ctypes.Structure):
         ("max_rounds", ctypes.c_uint64), ("time_limit_seconds", ctypes.c_double),
         ("round_batch", ctypes.c_int32), ("bfs_batch", ctypes.c_int32),
         ("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-        ("work_relabel_factor", ctypes.c_double),
+        ("work_relabel_factor", ctypes.c_double), ("engine", ctypes.c_int32),
     ]
 
 
