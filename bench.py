@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-tets", type=float, default=8e6)
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-graph batch (config 3)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving loop (config 5)")
+    ap.add_argument("--serve-seconds", type=float, default=8.0)
     return ap.parse_args()
 
 
@@ -237,14 +240,20 @@ def run_ours(args, world, rank, local):
     ms_max = max_over_ranks(ms, world)
     clocks = clk.summary()
 
-    # roofline of the dominant phase, from the same timed steps
+    # roofline of the dominant kernel, from the same timed steps
     dis_ms = sum(s["discharge_ms"] for s in stats)
     bfs_ms = sum(s["bfs_ms"] for s in stats)
     visits = sum(s["node_visits"] for s in stats)
     pushes = sum(s["pushes"] for s in stats)
     bfsv = sum(s["bfs_visits"] for s in stats)
     pk, pk_kind = peaks()
-    if dis_ms >= bfs_ms:
+    if int(stats[-1]["engine"]) == 2:
+        # persistent engine: one cooperative launch holds every round and
+        # every BFS level; its duration is the solve's device time
+        kern = "k_solve_persistent"
+        nbytes = B_VISIT * visits + B_PUSH * pushes + B_BFS * bfsv
+        kms, launches = sum(s["solve_device_ms"] for s in stats), len(stats)
+    elif dis_ms >= bfs_ms:
         kern = "k_discharge"
         nbytes = B_VISIT * visits + B_PUSH * pushes
         kms, launches = dis_ms, sum(s["discharge_launches"] for s in stats)
@@ -266,8 +275,8 @@ def run_ours(args, world, rank, local):
                 "algorithmic_bytes_per_step": int(nbytes / args.steps),
                 "kernel_ms_per_step": round(kms / args.steps, 3),
                 "launches_per_step": int(launches / args.steps),
-                "phase_ms_per_step": {"discharge": round(dis_ms / args.steps, 3),
-                                      "bfs": round(bfs_ms / args.steps, 3),
+                "engine": int(stats[-1]["engine"]),
+                "phase_ms_per_step": {"solve": round(sum(s["solve_device_ms"] for s in stats) / args.steps, 3),
                                       "build": round(sum(s["build_device_ms"] for s in stats) / args.steps, 3)}}
 
     # e2e through the drop-in module: pinned host topology, host V/labels
@@ -306,6 +315,8 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, args.seed)
+    batch = run_batch(args, local) if rank == 0 and not args.no_batch else None
+    serve = run_serve(args) if rank == 0 and not args.no_serve else None
 
     s0 = stats[-1]
     line = {
@@ -324,9 +335,142 @@ def run_ours(args, world, rank, local):
                   "pushes": int(s0["pushes"]), "solve_device_ms": round(s0["solve_device_ms"], 3),
                   "build_device_ms": round(s0["build_device_ms"], 3)},
         "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+        "batch": batch, "serve": serve,
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
     }
     return line
+
+
+def run_batch(args, local):
+    """Config 3: 64 uneven graphs (tets log-uniform 50k..4M) cut as one batch
+    vs the same 64 graphs cut one after the other, inputs in HBM."""
+    import torch
+
+    import gpupr_capi
+    import synth
+
+    dev = torch.device("cuda", local)
+    sizes = synth.config3_sizes(args.seed, 64)
+    graphs = [synth.config3_graph(i, int(n), args.seed) for i, n in enumerate(sizes)]
+    toff, voff, V, T, Nb, L = gpupr_capi.pack_batch(graphs)
+    t, nb, v, l = (torch.from_numpy(x).to(dev) for x in (T, Nb, V, L))
+    out = torch.empty(len(L), dtype=torch.uint8, device=dev)
+    singles = [tuple(torch.from_numpy(np.ascontiguousarray(g[k])).to(dev)
+                     for k in ("tets", "neighbors", "vertices", "labels")) for g in graphs]
+    outs = [torch.empty(len(g["labels"]), dtype=torch.uint8, device=dev) for g in graphs]
+    stream = torch.cuda.current_stream(dev)
+    gpupr_capi.graph_cut_batch(toff, voff, v, t, nb, l, 10.0, out=out)
+    for (gt, gn, gv, gl), o in zip(singles, outs):
+        gpupr_capi.graph_cut(gv, gt, gn, gl, 10.0, out=o)
+    torch.cuda.synchronize()
+    reps = 3
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        _, items, bst = gpupr_capi.graph_cut_batch(toff, voff, v, t, nb, l, 10.0, out=out)
+    b.record(stream)
+    torch.cuda.synchronize()
+    batch_ms = a.elapsed_time(b) / reps
+    a.record(stream)
+    seq = []
+    for (gt, gn, gv, gl), o in zip(singles, outs):
+        _, st = gpupr_capi.graph_cut(gv, gt, gn, gl, 10.0, out=o)
+        seq.append(st)
+    b.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = a.elapsed_time(b)
+    same = all(items[k]["adjusted_flow"] == seq[k]["adjusted_flow"] for k in range(len(graphs)))
+    ob = out.cpu().numpy()
+    same = same and all(np.array_equal(ob[int(toff[k]):int(toff[k + 1])], outs[k].cpu().numpy())
+                        for k in range(len(graphs)))
+    return {"config": "64 graphs, tets log-uniform 50k..4M (holed icosphere / holed torus / "
+                      "open rounded box, Kuhn lattices), lambda_fill=10, inputs in HBM",
+            "graphs": len(graphs), "tets": int(toff[-1]), "batch_ms": round(batch_ms, 3),
+            "sequential_ms": round(seq_ms, 3), "speedup": round(seq_ms / batch_ms, 2),
+            "batched_cuts_per_s": round(len(graphs) / (batch_ms * 1e-3), 1),
+            "sequential_cuts_per_s": round(len(graphs) / (seq_ms * 1e-3), 1),
+            "identical_to_sequential": bool(same), "engine": int(bst["engine"]),
+            "rounds": int(bst["rounds"]), "global_relabels": int(bst["global_relabels"])}
+
+
+def run_serve(args):
+    """Config 5: Poisson arrivals at 20 req/s, tets log-uniform 100k..20M,
+    160 GiB admission budget; continuous batching server vs one-at-a-time
+    FIFO service (simulated on the same arrival trace from measured
+    per-request service times)."""
+    import threading
+
+    import torch
+
+    import gpupr_capi
+    import synth
+
+    rng = np.random.default_rng(args.seed + 5)
+    pool_sizes = np.exp(rng.uniform(np.log(1e5), np.log(2e7), size=12)).astype(np.int64)
+    pool = [synth.config3_graph(i, int(n), args.seed + 5) for i, n in enumerate(pool_sizes)]
+    # service time of each pool graph alone (host inputs in, labels out)
+    service = []
+    for g in pool:
+        t_ = torch.from_numpy(g["tets"]).cuda()
+        n_ = torch.from_numpy(g["neighbors"]).cuda()
+        gpupr_capi.graph_cut(g["vertices"], t_, n_, g["labels"], 10.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tt = torch.from_numpy(g["tets"]).cuda()
+        nn = torch.from_numpy(g["neighbors"]).cuda()
+        gpupr_capi.graph_cut(g["vertices"], tt, nn, g["labels"], 10.0)
+        torch.cuda.synchronize()
+        service.append(time.perf_counter() - t0)
+        del t_, n_, tt, nn
+    n_req = int(20 * args.serve_seconds)
+    gaps = rng.exponential(1 / 20.0, size=n_req)
+    arrivals = np.cumsum(gaps)
+    picks = rng.integers(len(pool), size=n_req)
+    results = {}
+    with gpupr_capi.Server(hbm_budget_bytes=160 << 30) as sv:
+        rid0 = sv.submit(pool[0]["vertices"], pool[0]["tets"], pool[0]["neighbors"], pool[0]["labels"])
+        sv.wait(rid0)
+        ids = []
+        t_start = time.perf_counter()
+
+        def submitter():
+            for k in range(n_req):
+                delay = arrivals[k] - (time.perf_counter() - t_start)
+                if delay > 0:
+                    time.sleep(delay)
+                g = pool[picks[k]]
+                ids.append((k, sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"])))
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        done = 0
+        while done < n_req:
+            while len(ids) <= done:
+                time.sleep(0.001)
+            k, rid = ids[done]
+            _, res = sv.wait(rid)
+            results[k] = res
+            done += 1
+        th.join()
+        wall = time.perf_counter() - t_start
+    lat = np.array([results[k]["latency_ms"] for k in range(n_req)])
+    bs = np.array([results[k]["batch_size"] for k in range(n_req)])
+    # FIFO one-at-a-time service on the same trace
+    free_at, seq_lat = 0.0, []
+    for k in range(n_req):
+        start = max(arrivals[k], free_at)
+        free_at = start + service[picks[k]]
+        seq_lat.append(1e3 * (free_at - arrivals[k]))
+    seq_lat = np.array(seq_lat)
+    return {"config": "Poisson 20 req/s for %.0f s, tets log-uniform 100k..20M (pool of 12 "
+                      "seeded graphs), 160 GiB budget" % args.serve_seconds,
+            "requests": n_req, "p50_ms": round(float(np.percentile(lat, 50)), 2),
+            "p99_ms": round(float(np.percentile(lat, 99)), 2),
+            "cuts_per_s": round(n_req / wall, 2), "mean_batch": round(float(bs.mean()), 2),
+            "max_batch": int(bs.max()),
+            "sequential_fifo_p50_ms": round(float(np.percentile(seq_lat, 50)), 2),
+            "sequential_fifo_p99_ms": round(float(np.percentile(seq_lat, 99)), 2),
+            "mean_tets_per_request": int(np.mean([len(pool[p]["labels"]) for p in picks]))}
 
 
 def run_reference(args, world, rank, local):

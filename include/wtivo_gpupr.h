@@ -135,6 +135,69 @@ gpupr_status gpupr_graph_cut_ex(const double* vertices, uint64_t n_vertices,
                                 uint8_t* out_labels, int out_on_device,
                                 void* stream, gpupr_cut_stats* stats);
 
+/* One graph of a batch: its flows and sizes. */
+typedef struct {
+    int64_t adjusted_flow;   /* max flow of this graph (raw + terminal base flow) */
+    int64_t raw_flow;
+    uint64_t n_tets;
+    uint64_t free_n;
+} gpupr_batch_item;
+
+/*
+ * Batched graph cut: n_graphs independent cell graphs cut in one solve.
+ * No counterpart in the reference (it cuts one graph per call).  The graphs
+ * are packed end to end: graph g owns tets [tet_offsets[g], tet_offsets[g+1])
+ * and vertices [vertex_offsets[g], vertex_offsets[g+1]) of the concatenated
+ * arrays, and its tets/neighbors use LOCAL ids (0-based within the graph,
+ * -1 = hull), exactly what graph_cut_fast takes for one graph.  Offsets are
+ * host arrays of n_graphs+1 entries starting at 0.  out_labels is the
+ * concatenation of every graph's graph_cut_fast labels; items[g] receives
+ * each graph's flows.  One fill_T and one set of options for the batch.
+ */
+gpupr_status gpupr_graph_cut_batch(uint32_t n_graphs, const uint64_t* tet_offsets,
+                                   const uint64_t* vertex_offsets, const double* vertices,
+                                   int vertices_on_device, const int32_t* d_tets,
+                                   const int32_t* d_neighbors, const uint8_t* labels,
+                                   int labels_on_device, double fill_T,
+                                   const gpupr_solve_options* options, uint8_t* out_labels,
+                                   int out_on_device, void* stream, gpupr_batch_item* items,
+                                   gpupr_cut_stats* stats);
+
+/*
+ * Serving loop (continuous batching).  No counterpart in the reference.
+ * A server owns a worker thread on the device current at creation.  Requests
+ * (one cell graph each, HOST arrays with graph_cut_fast's layout, copied at
+ * submit) are admitted in arrival order while their estimated device
+ * footprint fits hbm_budget_bytes (0 = 160 GiB), cut together as one batch,
+ * and their results kept until gpupr_server_wait() reads them out.  Requests
+ * that arrive while a batch runs join the next one.
+ */
+typedef struct gpupr_server gpupr_server;
+typedef struct {
+    uint64_t id;
+    int32_t status;           /* gpupr_status of the request */
+    int32_t batch_size;       /* requests cut in the same batch */
+    int64_t adjusted_flow;
+    int64_t raw_flow;
+    uint64_t n_tets;
+    uint64_t free_n;
+    double queue_ms;          /* submit -> admitted */
+    double solve_ms;          /* the batch's device work, uploads included */
+    double latency_ms;        /* submit -> result ready */
+} gpupr_request_result;
+
+gpupr_status gpupr_server_create(uint64_t hbm_budget_bytes, const gpupr_solve_options* options,
+                                 gpupr_server** server);
+gpupr_status gpupr_server_submit(gpupr_server* server, const double* vertices,
+                                 uint64_t n_vertices, const int32_t* tets,
+                                 const int32_t* neighbors, const uint8_t* labels,
+                                 uint64_t n_tets, double fill_T, uint64_t* request_id);
+/* Blocks until the request is done (or timeout_s, > 0, passes): copies its
+ * labels to out_labels (host, n_tets bytes; may be NULL) and releases it. */
+gpupr_status gpupr_server_wait(gpupr_server* server, uint64_t request_id, double timeout_s,
+                               uint8_t* out_labels, gpupr_request_result* result);
+gpupr_status gpupr_server_destroy(gpupr_server* server);
+
 /*
  * Reduced-graph build only (bindings.cpp:146-314): writes the reference's
  * host arrays so the build can be compared byte for byte.  All outputs are

@@ -1,0 +1,62 @@
+"""Serving loop: a result is the same alone and in the mix."""
+from __future__ import annotations
+
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import cached_graph
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _pool():
+    return [cached_graph("proxy", 0, 20_000), cached_graph("lattice", 2, 80_000),
+            cached_graph("box", 4, 60_000), cached_graph("torus", 5, 60_000)]
+
+
+def test_results_same_alone_and_in_the_mix(built):
+    import gpupr_capi
+
+    pool = _pool()
+    want = [orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0) for g in pool]
+    with gpupr_capi.Server() as sv:
+        # alone: one request at a time
+        for g, (lab, st) in zip(pool, want):
+            rid = sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"])
+            out, res = sv.wait(rid, timeout_s=120)
+            assert np.array_equal(out, lab) and res["adjusted_flow"] == st["adjusted_flow"]
+        # in the mix: submitted together from several threads, repeated
+        ids = {}
+
+        def client(k):
+            for rep in range(3):
+                g = pool[(k + rep) % len(pool)]
+                ids[(k, rep)] = ((k + rep) % len(pool),
+                                 sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"]))
+
+        ts = [threading.Thread(target=client, args=(k,)) for k in range(4)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        sizes = []
+        for (k, rep), (gi, rid) in ids.items():
+            out, res = sv.wait(rid, timeout_s=120)
+            lab, st = want[gi]
+            assert np.array_equal(out, lab), (k, rep)
+            assert res["adjusted_flow"] == st["adjusted_flow"] and res["status"] == 0
+            assert res["latency_ms"] >= res["queue_ms"] >= 0
+            sizes.append(res["batch_size"])
+        assert max(sizes) > 1          # requests really were batched together
+
+
+def test_oversized_request_refused(built):
+    import gpupr_capi
+
+    g = _pool()[0]
+    with gpupr_capi.Server(hbm_budget_bytes=1 << 20) as sv:
+        with pytest.raises(gpupr_capi.GpuprError):
+            sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"])

@@ -15,6 +15,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "gpupr_internal.cuh"
 #include "wtivo_gpupr.h"
@@ -223,6 +224,125 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
 
 }  // namespace
 
+void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
+                         const double* vertices, int v_dev, const int32_t* d_tets_l,
+                         const int32_t* d_nbrs_l, const uint8_t* labels, int l_dev, double fill_T,
+                         const gpupr_solve_options* options, uint8_t* out, int out_dev,
+                         cudaStream_t s, gpupr_batch_item* items, gpupr_cut_stats* st)
+{
+    const auto all0 = std::chrono::steady_clock::now();
+    if (!st || !items || !toff || !voff) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL batch argument"};
+    std::memset(st, 0, sizeof(*st));
+    std::memset(items, 0, sizeof(gpupr_batch_item) * G);
+    if (!G) return;
+    if (toff[0] != 0 || voff[0] != 0) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "batch offsets must start at 0"};
+    for (uint32_t g = 0; g < G; ++g) {
+        if (toff[g + 1] < toff[g] || voff[g + 1] < voff[g])
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "batch offsets must be non-decreasing"};
+        items[g].n_tets = toff[g + 1] - toff[g];
+    }
+    const uint64_t N = toff[G], nv = voff[G];
+    st->n_full = N;
+    st->threads = 1;
+    st->local_steps = options && options->local_steps ? options->local_steps : 8;
+    if (N > 0x7FFFFFFEull) throw Error{GPUPR_ERR_TOO_MANY_TETS, "batch exceeds 2^31-1 tets"};
+    if (N == 0) return;
+    if (!d_tets_l || !d_nbrs_l || !labels || !out || (!vertices && nv))
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL batch array"};
+    if (!aligned(d_tets_l, 16) || !aligned(d_nbrs_l, 16))
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets/neighbors must be 16-byte aligned"};
+    select_device_for(d_tets_l, "tets/neighbors");
+    uint64_t launches = 0;
+
+    const auto b0 = std::chrono::steady_clock::now();
+    Timer tb(s);
+    DevBuf<uint8_t> dlab;
+    DevBuf<double> dver;
+    const uint8_t* d_labels = on_device(labels, N, l_dev, dlab, s);
+    const double* d_vertices = on_device(vertices, nv * 3u, v_dev, dver, s);
+    DevBuf<unsigned long long> d_toff(G + 1, s), d_voff(G + 1, s);
+    GPUPR_CUDA(cudaMemcpyAsync(d_toff.p, toff, (G + 1) * 8u, cudaMemcpyHostToDevice, s));
+    GPUPR_CUDA(cudaMemcpyAsync(d_voff.p, voff, (G + 1) * 8u, cudaMemcpyHostToDevice, s));
+    DevBuf<int32_t> gt(N * 4u, s), gn(N * 4u, s);
+    batch_pack(N, G, d_toff.p, d_voff.p, d_tets_l, d_nbrs_l, gt.p, gn.p, s, &launches);
+
+    BuildInputs in{d_vertices, nv, gt.p, gn.p, d_labels, N, fill_T};
+    in.want_base_node = true;
+    ReducedGraph g;
+    BuildInfo info;
+    build_reduced_graph(in, g, info, s, &launches);
+    st->build_device_ms = tb.stop_ms();
+    st->build_seconds = seconds_since(b0);
+    st->full_E = info.full_refs / 2u;
+    st->fixed_source = info.fixed_source;
+    st->fixed_sink = info.fixed_sink;
+    st->free_n = info.free_n;
+    if (info.free_n == 0) {
+        if (out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, d_labels, N, cudaMemcpyDeviceToDevice, s));
+        else GPUPR_CUDA(cudaMemcpyAsync(out, d_labels, N, cudaMemcpyDeviceToHost, s));
+        GPUPR_CUDA(cudaStreamSynchronize(s));
+        st->kernel_launches = launches;
+        st->native_total_seconds = seconds_since(all0);
+        return;
+    }
+    const SolveOptions opt = resolve_options(options, 8, 1024, 2000000ull);
+    SolveWorkspace w;
+    SolveResult sr;
+    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.term.p, w, opt, s, sr);
+    launches += sr.launches;
+
+    DevBuf<uint8_t> dout;
+    uint8_t* d_out = out;
+    if (!out_dev) {
+        dout = DevBuf<uint8_t>(N, s);
+        d_out = dout.p;
+    }
+    GPUPR_CUDA(cudaMemcpyAsync(d_out, d_labels, N, cudaMemcpyDeviceToDevice, s));
+    scatter_partition(g.n, g.free_old.p, w.height.p, d_out, s, &launches);
+
+    // per-graph flows over each graph's contiguous free-node range
+    DevBuf<unsigned long long> counts(G, s), d_foff(G + 1, s), base(G, s);
+    DevBuf<long long> raw(G, s);
+    batch_free_counts(G, d_toff.p, g.full_to_free.p, counts.p, s, &launches);
+    std::vector<unsigned long long> hc(G), hfo(G + 1), hb(G);
+    std::vector<long long> hr(G);
+    GPUPR_CUDA(cudaMemcpyAsync(hc.data(), counts.p, G * 8u, cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    hfo[0] = 0;
+    for (uint32_t k = 0; k < G; ++k) hfo[k + 1] = hfo[k] + hc[k];
+    GPUPR_CUDA(cudaMemcpyAsync(d_foff.p, hfo.data(), (G + 1) * 8u, cudaMemcpyHostToDevice, s));
+    batch_flows(G, d_foff.p, g.term.p, w.excess.p, g.base_node.p, raw.p, base.p, s, &launches);
+    GPUPR_CUDA(cudaMemcpyAsync(hr.data(), raw.p, G * 8u, cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaMemcpyAsync(hb.data(), base.p, G * 8u, cudaMemcpyDeviceToHost, s));
+    if (!out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, d_out, N, cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t k = 0; k < G; ++k) {
+        items[k].raw_flow = hr[k];
+        items[k].adjusted_flow = hr[k] + (long long)hb[k];
+        items[k].free_n = hc[k];
+    }
+    st->raw_flow = sr.raw_flow;
+    st->adjusted_flow = sr.raw_flow + info.terminal_base_flow;
+    st->graph_bytes = g.graph_bytes();
+    st->workspace_bytes = sr.workspace_bytes;
+    st->free_E = info.free_refs / 2u;
+    st->terminal_edges = info.terminal_edges;
+    st->rounds = sr.rounds;
+    st->global_relabels = sr.relabels;
+    st->map_bytes = N * 4u + (uint64_t)g.n * 4u;
+    st->solve_seconds = sr.solve_s;
+    st->node_visits = sr.node_visits;
+    st->pushes = sr.pushes;
+    st->bfs_visits = sr.bfs_visits;
+    st->bfs_levels = sr.bfs_levels;
+    st->solve_device_ms = sr.solve_device_ms;
+    st->discharge_ms = sr.discharge_ms;
+    st->bfs_ms = sr.bfs_ms;
+    st->engine = sr.engine;
+    st->kernel_launches = launches;
+    st->native_total_seconds = seconds_since(all0);
+}
+
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 void* pool_alloc(size_t bytes, cudaStream_t s)
@@ -303,6 +423,23 @@ gpupr_status gpupr_graph_cut_ex(const double* vertices, uint64_t n_vertices, int
         run_graph_cut(vertices, n_vertices, vertices_on_device, d_tets, d_neighbors, n_tets, labels,
                       labels_on_device, fill_T, threads, per, mr, ls, options, out_labels,
                       out_on_device, static_cast<cudaStream_t>(stream), stats);
+    });
+}
+
+gpupr_status gpupr_graph_cut_batch(uint32_t n_graphs, const uint64_t* tet_offsets,
+                                   const uint64_t* vertex_offsets, const double* vertices,
+                                   int vertices_on_device, const int32_t* d_tets,
+                                   const int32_t* d_neighbors, const uint8_t* labels,
+                                   int labels_on_device, double fill_T,
+                                   const gpupr_solve_options* options, uint8_t* out_labels,
+                                   int out_on_device, void* stream, gpupr_batch_item* items,
+                                   gpupr_cut_stats* stats)
+{
+    return guarded([&] {
+        run_graph_cut_batch(n_graphs, tet_offsets, vertex_offsets, vertices, vertices_on_device,
+                            d_tets, d_neighbors, labels, labels_on_device, fill_T, options,
+                            out_labels, out_on_device, static_cast<cudaStream_t>(stream), items,
+                            stats);
     });
 }
 

@@ -122,6 +122,7 @@ struct BuildInputs {
     const uint8_t* d_labels;    // device [N]
     uint64_t N;
     double fill_T;
+    bool want_base_node = false;       // also keep min(src, snk) per free node
 };
 
 struct BuildInfo {
@@ -138,12 +139,25 @@ struct ReducedGraph {
     DevBuf<int32_t> term;
     DevBuf<int32_t> full_to_free;  // N
     DevBuf<uint32_t> free_old;     // n
+    DevBuf<uint32_t> base_node;    // n, only when BuildInputs::want_base_node
     uint64_t graph_bytes() const { return nbr.bytes() + res.bytes() + rev.bytes() + term.bytes(); }
 };
 
 // Classify + compact + build; throws gpupr::Error with reference messages.
 void build_reduced_graph(const BuildInputs& in, ReducedGraph& g, BuildInfo& info,
                          cudaStream_t s, uint64_t* launches);
+
+// Batches (batch.cu): G graphs packed end to end.  Local vertex/neighbor ids
+// become global ids; per-graph sums run over contiguous ranges.
+void batch_pack(uint64_t N, uint32_t G, const unsigned long long* d_tet_off,
+                const unsigned long long* d_vert_off, const int32_t* d_tets_local,
+                const int32_t* d_nbrs_local, int32_t* d_tets, int32_t* d_nbrs, cudaStream_t s,
+                uint64_t* launches);
+void batch_free_counts(uint32_t G, const unsigned long long* d_tet_off, const int32_t* d_full_to_free,
+                       unsigned long long* d_counts, cudaStream_t s, uint64_t* launches);
+void batch_flows(uint32_t G, const unsigned long long* d_free_off, const int32_t* d_term,
+                 const long long* d_excess, const uint32_t* d_base_node, long long* d_raw,
+                 unsigned long long* d_base, cudaStream_t s, uint64_t* launches);
 
 // Exclusive scan of per-tile counts (one block); *d_total receives the sum.
 void scan_tile_counts(uint32_t ntiles, const uint32_t* d_cnt, unsigned long long* d_off,
@@ -222,6 +236,13 @@ void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t*
                            SolveResult& out);
 void compute_reverse_slots_noalloc(uint32_t n, const int4* d_nbr, uint8_t* d_rev, int32_t* d_err,
                                    cudaStream_t s);
+
+// Batched graph cut (capi.cu), used by the C ABI and the serving loop.
+void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
+                         const double* vertices, int v_dev, const int32_t* d_tets_l,
+                         const int32_t* d_nbrs_l, const uint8_t* labels, int l_dev, double fill_T,
+                         const gpupr_solve_options* options, uint8_t* out, int out_dev,
+                         cudaStream_t s, gpupr_batch_item* items, gpupr_cut_stats* st);
 
 // Bounded wait self test kernel driver.
 gpupr_status bounded_wait_selftest(uint32_t limit_us, cudaStream_t s);

@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(TPB) k_build_rows(
     const uint8_t* __restrict__ labels, const int32_t* __restrict__ full_to_free,
     const uint32_t* __restrict__ free_old, double fill_T, int4* __restrict__ out_nbr,
     uint4* __restrict__ out_res, uint8_t* __restrict__ out_rev, int32_t* __restrict__ out_term,
-    BuildCtl* ctl)
+    uint32_t* __restrict__ out_base, BuildCtl* ctl)
 {
     __shared__ unsigned long long sh[TPB / 32];
     unsigned long long refs = 0, terms = 0;
@@ -259,6 +259,7 @@ __global__ void __launch_bounds__(TPB) k_build_rows(
             atomicExch(&ctl->err_node, i);
         }
         base += (src < snk) ? src : snk;
+        if (out_base) out_base[q] = (uint32_t)((src < snk) ? src : snk);
         out_nbr[q] = make_int4(on[0], on[1], on[2], on[3]);
         out_res[q] = make_uint4(orr[0], orr[1], orr[2], orr[3]);
         out_rev[q] = (uint8_t)rv;
@@ -392,10 +393,12 @@ void build_reduced_graph(const BuildInputs& in, ReducedGraph& g, BuildInfo& info
     g.res = DevBuf<uint32_t>((size_t)F * 4u, s);
     g.rev = DevBuf<uint8_t>(F, s);
     g.term = DevBuf<int32_t>(F, s);
+    if (in.want_base_node) g.base_node = DevBuf<uint32_t>(F, s);
     k_build_rows<<<grid_for(F), TPB, 0, s>>>(
         F, N, in.d_vertices, in.nv, reinterpret_cast<const int4*>(in.d_tets),
         reinterpret_cast<const int4*>(in.d_nbrs), in.d_labels, g.full_to_free.p, g.free_old.p,
-        in.fill_T, g.nbr.p, reinterpret_cast<uint4*>(g.res.p), g.rev.p, g.term.p, ctl.p);
+        in.fill_T, g.nbr.p, reinterpret_cast<uint4*>(g.res.p), g.rev.p, g.term.p, g.base_node.p,
+        ctl.p);
     GPUPR_CUDA(cudaGetLastError());
     *launches += 1;
     GPUPR_CUDA(cudaMemcpyAsync(&h, ctl.p, sizeof(h), cudaMemcpyDeviceToHost, s));

@@ -55,6 +55,19 @@ class SolveOptions(ctypes.Structure):
     ]
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [("adjusted_flow", ctypes.c_int64), ("raw_flow", ctypes.c_int64),
+                ("n_tets", ctypes.c_uint64), ("free_n", ctypes.c_uint64)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int32), ("batch_size", ctypes.c_int32),
+                ("adjusted_flow", ctypes.c_int64), ("raw_flow", ctypes.c_int64),
+                ("n_tets", ctypes.c_uint64), ("free_n", ctypes.c_uint64),
+                ("queue_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double)]
+
+
 class GpuprError(RuntimeError):
     def __init__(self, status, message):
         super().__init__(message)
@@ -102,6 +115,13 @@ def lib():
         L.gpupr_surface_count.argtypes = [p, ctypes.c_int, p, u64, ctypes.c_int, p, p, u64, p, p, p]
         L.gpupr_surface_fetch.argtypes = [p, p, ctypes.c_int, p]
         L.gpupr_solve_reduced_noalloc.argtypes = [ctypes.c_uint32, p, p, p, p, i32, u64, i32, p, p]
+        L.gpupr_graph_cut_batch.argtypes = [ctypes.c_uint32, p, p, p, ctypes.c_int, p, p, p,
+                                            ctypes.c_int, f64, p, p, ctypes.c_int, p, p, p]
+        L.gpupr_server_create.argtypes = [ctypes.c_uint64, p, ctypes.POINTER(p)]
+        L.gpupr_server_submit.argtypes = [p, p, ctypes.c_uint64, p, p, p, ctypes.c_uint64, f64,
+                                          ctypes.POINTER(ctypes.c_uint64)]
+        L.gpupr_server_wait.argtypes = [p, ctypes.c_uint64, f64, p, p]
+        L.gpupr_server_destroy.argtypes = [p]
         L.gpupr_release_cached_memory.argtypes = []
         L.gpupr_selftest_bounded_wait.argtypes = [ctypes.c_uint32, p]
         for name in header_functions():
@@ -174,6 +194,97 @@ def graph_cut(vertices, tets, nbrs, labels, fill_T, threads=16, global_relabel_p
                                       int(o_dev), _stream(torch, tets.device), ctypes.byref(st))
     check(rc)
     return out, st.as_dict()
+
+
+def pack_batch(graphs):
+    """Concatenate graphs (dicts with vertices/tets/neighbors/labels, local
+    ids) -> (tet_offsets, vertex_offsets, vertices, tets, neighbors, labels)."""
+    toff = np.zeros(len(graphs) + 1, np.uint64)
+    voff = np.zeros(len(graphs) + 1, np.uint64)
+    for k, g in enumerate(graphs):
+        toff[k + 1] = toff[k] + len(g["tets"])
+        voff[k + 1] = voff[k] + len(g["vertices"])
+    V = np.ascontiguousarray(np.concatenate([g["vertices"] for g in graphs]), np.float64)
+    T = np.ascontiguousarray(np.concatenate([g["tets"] for g in graphs]), np.int32)
+    Nb = np.ascontiguousarray(np.concatenate([g["neighbors"] for g in graphs]), np.int32)
+    L = np.ascontiguousarray(np.concatenate([g["labels"] for g in graphs]), np.uint8)
+    return toff, voff, V, T, Nb, L
+
+
+def graph_cut_batch(toff, voff, vertices, tets, nbrs, labels, fill_T, opts=None, out=None):
+    """gpupr_graph_cut_batch.  tets/nbrs: CUDA int32 tensors (local ids,
+    concatenated); vertices/labels numpy or CUDA.  Returns (labels_out,
+    items list of dicts, stats dict)."""
+    import torch
+
+    G = len(toff) - 1
+    toff = np.ascontiguousarray(toff, np.uint64)
+    voff = np.ascontiguousarray(voff, np.uint64)
+    v_dev = isinstance(vertices, torch.Tensor)
+    l_dev = isinstance(labels, torch.Tensor)
+    N = int(toff[-1])
+    if out is None:
+        out = torch.empty(N, dtype=torch.uint8, device=tets.device) if l_dev else np.empty(N, np.uint8)
+    o_dev = isinstance(out, torch.Tensor)
+    if not v_dev:
+        vertices = np.ascontiguousarray(vertices, np.float64)
+    if not l_dev:
+        labels = np.ascontiguousarray(labels, np.uint8)
+    items = (BatchItem * max(G, 1))()
+    st = CutStats()
+    check(lib().gpupr_graph_cut_batch(
+        G, _hp(toff), _hp(voff), _dp(vertices) if v_dev else _hp(vertices), int(v_dev), _dp(tets),
+        _dp(nbrs), _dp(labels) if l_dev else _hp(labels), int(l_dev), float(fill_T),
+        ctypes.byref(opts) if opts is not None else None, _dp(out) if o_dev else _hp(out), int(o_dev),
+        _stream(torch, tets.device), items, ctypes.byref(st)))
+    return out, [{k: getattr(items[i], k) for k, _ in BatchItem._fields_} for i in range(G)], st.as_dict()
+
+
+class Server:
+    """Continuous-batching cut server (gpupr_server_*): submit() host graphs
+    at any time, wait() for each result."""
+
+    def __init__(self, hbm_budget_bytes=0, opts=None):
+        import torch
+
+        torch.cuda.init()
+        lib()
+        self._h = ctypes.c_void_p()
+        check(_lib.gpupr_server_create(int(hbm_budget_bytes),
+                                       ctypes.byref(opts) if opts is not None else None,
+                                       ctypes.byref(self._h)))
+        self._n = {}
+
+    def submit(self, vertices, tets, nbrs, labels, fill_T=10.0):
+        V = np.ascontiguousarray(vertices, np.float64)
+        T = np.ascontiguousarray(tets, np.int32)
+        Nb = np.ascontiguousarray(nbrs, np.int32)
+        L = np.ascontiguousarray(labels, np.uint8)
+        rid = ctypes.c_uint64(0)
+        check(_lib.gpupr_server_submit(self._h, _hp(V), len(V), _hp(T), _hp(Nb), _hp(L), len(L),
+                                       float(fill_T), ctypes.byref(rid)))
+        self._n[rid.value] = len(L)
+        return rid.value
+
+    def wait(self, rid, timeout_s=0.0):
+        out = np.empty(max(self._n[rid], 1), np.uint8)
+        res = RequestResult()
+        rc = _lib.gpupr_server_wait(self._h, ctypes.c_uint64(rid), float(timeout_s), _hp(out),
+                                    ctypes.byref(res))
+        n = self._n.pop(rid)
+        check(rc)
+        return out[:n], {k: getattr(res, k) for k, _ in RequestResult._fields_}
+
+    def close(self):
+        if self._h:
+            _lib.gpupr_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def build_reduced(vertices, tets, nbrs, labels, fill_T):
