@@ -395,9 +395,11 @@ def run_batch(args, local):
 
 def run_serve(args):
     """Config 5: Poisson arrivals at 20 req/s, tets log-uniform 100k..20M,
-    160 GiB admission budget; continuous batching server vs one-at-a-time
-    FIFO service (simulated on the same arrival trace from measured
-    per-request service times)."""
+    160 GiB admission budget.  The same arrival trace goes through the
+    continuous-batching server, through the same server one request at a time
+    (max_batch 1: FIFO, uploads still overlapping the previous cut), and is
+    replayed against one-at-a-time service times measured alone (host arrays
+    copied in, cut, labels copied out: the naive FIFO)."""
     import threading
 
     import torch
@@ -408,54 +410,63 @@ def run_serve(args):
     rng = np.random.default_rng(args.seed + 5)
     pool_sizes = np.exp(rng.uniform(np.log(1e5), np.log(2e7), size=12)).astype(np.int64)
     pool = [synth.config3_graph(i, int(n), args.seed + 5) for i, n in enumerate(pool_sizes)]
-    # service time of each pool graph alone (host inputs in, labels out)
+    n_req = int(20 * args.serve_seconds)
+    arrivals = np.cumsum(rng.exponential(1 / 20.0, size=n_req))
+    picks = rng.integers(len(pool), size=n_req)
+
+    # service time of each pool graph alone: host topology -> device, cut, labels out
     service = []
     for g in pool:
-        t_ = torch.from_numpy(g["tets"]).cuda()
-        n_ = torch.from_numpy(g["neighbors"]).cuda()
-        gpupr_capi.graph_cut(g["vertices"], t_, n_, g["labels"], 10.0)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        tt = torch.from_numpy(g["tets"]).cuda()
-        nn = torch.from_numpy(g["neighbors"]).cuda()
-        gpupr_capi.graph_cut(g["vertices"], tt, nn, g["labels"], 10.0)
-        torch.cuda.synchronize()
-        service.append(time.perf_counter() - t0)
-        del t_, n_, tt, nn
-    n_req = int(20 * args.serve_seconds)
-    gaps = rng.exponential(1 / 20.0, size=n_req)
-    arrivals = np.cumsum(gaps)
-    picks = rng.integers(len(pool), size=n_req)
-    results = {}
-    with gpupr_capi.Server(hbm_budget_bytes=160 << 30) as sv:
-        rid0 = sv.submit(pool[0]["vertices"], pool[0]["tets"], pool[0]["neighbors"], pool[0]["labels"])
-        sv.wait(rid0)
-        ids = []
-        t_start = time.perf_counter()
+        for rep in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tt = torch.from_numpy(g["tets"]).cuda()
+            nn = torch.from_numpy(g["neighbors"]).cuda()
+            gpupr_capi.graph_cut(g["vertices"], tt, nn, g["labels"], 10.0)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            del tt, nn
+        service.append(dt)
 
-        def submitter():
-            for k in range(n_req):
-                delay = arrivals[k] - (time.perf_counter() - t_start)
-                if delay > 0:
-                    time.sleep(delay)
-                g = pool[picks[k]]
-                ids.append((k, sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"])))
+    def trace(max_batch):
+        results = {}
+        with gpupr_capi.Server(hbm_budget_bytes=160 << 30, max_batch=max_batch) as sv:
+            g0 = pool[0]
+            sv.wait(sv.submit(g0["vertices"], g0["tets"], g0["neighbors"], g0["labels"]))
+            ids = []
+            t_start = time.perf_counter()
 
-        th = threading.Thread(target=submitter)
-        th.start()
-        done = 0
-        while done < n_req:
-            while len(ids) <= done:
-                time.sleep(0.001)
-            k, rid = ids[done]
-            _, res = sv.wait(rid)
-            results[k] = res
-            done += 1
-        th.join()
-        wall = time.perf_counter() - t_start
-    lat = np.array([results[k]["latency_ms"] for k in range(n_req)])
-    bs = np.array([results[k]["batch_size"] for k in range(n_req)])
-    # FIFO one-at-a-time service on the same trace
+            def submitter():
+                for k in range(n_req):
+                    delay = arrivals[k] - (time.perf_counter() - t_start)
+                    if delay > 0:
+                        time.sleep(delay)
+                    g = pool[picks[k]]
+                    ids.append((k, sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"])))
+
+            th = threading.Thread(target=submitter)
+            th.start()
+            done = 0
+            while done < n_req:
+                while len(ids) <= done:
+                    time.sleep(0.0005)
+                k, rid = ids[done]
+                results[k] = sv.wait(rid)[1]
+                done += 1
+            th.join()
+            wall = time.perf_counter() - t_start
+        lat = np.array([results[k]["latency_ms"] for k in range(n_req)])
+        bs = np.array([results[k]["batch_size"] for k in range(n_req)])
+        up = np.array([results[k]["upload_ms"] for k in range(n_req)])
+        sv_ms = np.array([results[k]["solve_ms"] for k in range(n_req)])
+        return {"p50_ms": round(float(np.percentile(lat, 50)), 2),
+                "p99_ms": round(float(np.percentile(lat, 99)), 2),
+                "cuts_per_s": round(n_req / wall, 2), "mean_batch": round(float(bs.mean()), 2),
+                "max_batch": int(bs.max()), "mean_upload_ms": round(float(up.mean()), 2),
+                "mean_solve_ms": round(float(sv_ms.mean()), 2)}
+
+    batched = trace(0)
+    one_at_a_time = trace(1)
     free_at, seq_lat = 0.0, []
     for k in range(n_req):
         start = max(arrivals[k], free_at)
@@ -463,14 +474,13 @@ def run_serve(args):
         seq_lat.append(1e3 * (free_at - arrivals[k]))
     seq_lat = np.array(seq_lat)
     return {"config": "Poisson 20 req/s for %.0f s, tets log-uniform 100k..20M (pool of 12 "
-                      "seeded graphs), 160 GiB budget" % args.serve_seconds,
-            "requests": n_req, "p50_ms": round(float(np.percentile(lat, 50)), 2),
-            "p99_ms": round(float(np.percentile(lat, 99)), 2),
-            "cuts_per_s": round(n_req / wall, 2), "mean_batch": round(float(bs.mean()), 2),
-            "max_batch": int(bs.max()),
-            "sequential_fifo_p50_ms": round(float(np.percentile(seq_lat, 50)), 2),
-            "sequential_fifo_p99_ms": round(float(np.percentile(seq_lat, 99)), 2),
-            "mean_tets_per_request": int(np.mean([len(pool[p]["labels"]) for p in picks]))}
+                      "seeded graphs), 160 GiB budget, host arrays in and out" % args.serve_seconds,
+            "requests": n_req, "mean_tets_per_request": int(np.mean([len(pool[p]["labels"]) for p in picks])),
+            **batched,
+            "server_max_batch_1": one_at_a_time,
+            "naive_fifo": {"p50_ms": round(float(np.percentile(seq_lat, 50)), 2),
+                           "p99_ms": round(float(np.percentile(seq_lat, 99)), 2),
+                           "mean_service_ms": round(1e3 * float(np.mean([service[p] for p in picks])), 2)}}
 
 
 def run_reference(args, world, rank, local):

@@ -165,12 +165,16 @@ gpupr_status gpupr_graph_cut_batch(uint32_t n_graphs, const uint64_t* tet_offset
 
 /*
  * Serving loop (continuous batching).  No counterpart in the reference.
- * A server owns a worker thread on the device current at creation.  Requests
- * (one cell graph each, HOST arrays with graph_cut_fast's layout, copied at
- * submit) are admitted in arrival order while their estimated device
- * footprint fits hbm_budget_bytes (0 = 160 GiB), cut together as one batch,
- * and their results kept until gpupr_server_wait() reads them out.  Requests
- * that arrive while a batch runs join the next one.
+ * A server owns two threads on the device current at creation: a stager that
+ * admits requests in arrival order while their estimated device footprint
+ * fits hbm_budget_bytes (0 = 160 GiB) next to the batch being solved and
+ * uploads them as one packed batch, and a solver that cuts each staged batch
+ * in one solve.  Requests that arrive while a batch runs join the next one.
+ * A request is one cell graph in HOST arrays with graph_cut_fast's layout;
+ * the server BORROWS them (no copy): vertices, tets, neighbors and labels
+ * must stay valid and unchanged, and out_labels (n_tets bytes) writable,
+ * until gpupr_server_wait() has returned for the request or the server is
+ * destroyed (destroy finishes every submitted request first).
  */
 typedef struct gpupr_server gpupr_server;
 typedef struct {
@@ -181,21 +185,26 @@ typedef struct {
     int64_t raw_flow;
     uint64_t n_tets;
     uint64_t free_n;
-    double queue_ms;          /* submit -> admitted */
-    double solve_ms;          /* the batch's device work, uploads included */
+    double queue_ms;          /* submit -> admitted into a batch */
+    double upload_ms;         /* the batch's host -> device copies */
+    double solve_ms;          /* the batch's cut, labels copied out */
     double latency_ms;        /* submit -> result ready */
 } gpupr_request_result;
 
-gpupr_status gpupr_server_create(uint64_t hbm_budget_bytes, const gpupr_solve_options* options,
-                                 gpupr_server** server);
+/* max_batch: most requests per batch (0 = no limit; 1 = one request at a
+ * time, uploads still overlapping the previous cut). */
+gpupr_status gpupr_server_create(uint64_t hbm_budget_bytes, uint32_t max_batch,
+                                 const gpupr_solve_options* options, gpupr_server** server);
 gpupr_status gpupr_server_submit(gpupr_server* server, const double* vertices,
                                  uint64_t n_vertices, const int32_t* tets,
                                  const int32_t* neighbors, const uint8_t* labels,
-                                 uint64_t n_tets, double fill_T, uint64_t* request_id);
-/* Blocks until the request is done (or timeout_s, > 0, passes): copies its
- * labels to out_labels (host, n_tets bytes; may be NULL) and releases it. */
+                                 uint64_t n_tets, double fill_T, uint8_t* out_labels,
+                                 uint64_t* request_id);
+/* Blocks until the request is done (or timeout_s, > 0, passes; the request
+ * then stays in flight), fills result and releases the request: its labels
+ * are in the out_labels array given at submit. */
 gpupr_status gpupr_server_wait(gpupr_server* server, uint64_t request_id, double timeout_s,
-                               uint8_t* out_labels, gpupr_request_result* result);
+                               gpupr_request_result* result);
 gpupr_status gpupr_server_destroy(gpupr_server* server);
 
 /*
@@ -294,6 +303,18 @@ gpupr_status gpupr_solve_reduced_noalloc(uint32_t n, int32_t* d_neighbors,
                                          int32_t global_relabel_period,
                                          uint64_t max_rounds, int32_t local_steps,
                                          void* stream, gpupr_cut_stats* stats);
+
+/*
+ * Topology upload (replaces wtivo.py:284-309, topology_to_cuda_chunked):
+ * copies an Nx4 integer matrix from HOST memory (int32 or int64 elements,
+ * elem_bytes 4 or 8; any byte strides, e.g. Fortran order) into a
+ * contiguous int32 Nx4 device array d_out (16-byte aligned), narrowing int64
+ * like numpy's astype(int32).  Returns once the host matrix has been read;
+ * d_out is ready in the order of `stream`.
+ */
+gpupr_status gpupr_upload_topology(const void* host, uint64_t rows, int64_t row_stride_bytes,
+                                   int64_t col_stride_bytes, int32_t elem_bytes, int32_t* d_out,
+                                   void* stream);
 
 /* Release device memory cached between calls (pool + scratch). */
 gpupr_status gpupr_release_cached_memory(void);

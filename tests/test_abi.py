@@ -93,3 +93,13 @@ def test_python_side_is_plumbing_only():
 
     src = inspect.getsource(gpupr_capi)
     assert "oracle" not in src.replace("no CPU fallback", "")
+
+
+def test_topology_upload_shape_check(built):
+    """wtivo.py:297-299: the shape is checked before anything is copied."""
+    import wtivo_gpupr
+
+    with pytest.raises(RuntimeError, match=r"tets: expected Nx4 topology array, got \(5, 3\)"):
+        wtivo_gpupr.topology_to_cuda_chunked(np.zeros((5, 3), np.int32), "tets")
+    with pytest.raises(RuntimeError, match=r"nb: expected Nx4 topology array, got \(8,\)"):
+        wtivo_gpupr.topology_to_cuda_chunked(np.zeros(8, np.int64), "nb")

@@ -60,3 +60,18 @@ def test_oversized_request_refused(built):
     with gpupr_capi.Server(hbm_budget_bytes=1 << 20) as sv:
         with pytest.raises(gpupr_capi.GpuprError):
             sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"])
+
+
+def test_destroy_finishes_submitted_requests(built):
+    import gpupr_capi
+
+    pool = _pool()
+    want = [orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0)[0] for g in pool]
+    sv = gpupr_capi.Server()
+    outs = []
+    for g in pool:
+        rid = sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"])
+        outs.append(sv._held[rid][4])
+    sv.close()                          # returns only after every request is cut
+    for out, lab in zip(outs, want):
+        assert np.array_equal(out[:len(lab)], lab)

@@ -93,10 +93,8 @@ double seconds_since(std::chrono::steady_clock::time_point t0)
 struct Timer {
     cudaEvent_t a = nullptr, b = nullptr;
     cudaStream_t s;
-    explicit Timer(cudaStream_t st) : s(st)
+    explicit Timer(cudaStream_t st) : a(timing_event(0)), b(timing_event(1)), s(st)
     {
-        GPUPR_CUDA(cudaEventCreate(&a));
-        GPUPR_CUDA(cudaEventCreate(&b));
         GPUPR_CUDA(cudaEventRecord(a, s));
     }
     double stop_ms()
@@ -107,11 +105,6 @@ struct Timer {
         GPUPR_CUDA(cudaEventElapsedTime(&ms, a, b));
         return ms;
     }
-    ~Timer()
-    {
-        if (a) cudaEventDestroy(a);
-        if (b) cudaEventDestroy(b);
-    }
 };
 
 // Device copies of host inputs (no copy when already on the device).
@@ -120,7 +113,7 @@ const T* on_device(const T* p, size_t count, int is_device, DevBuf<T>& keep, cud
 {
     if (is_device || count == 0) return p;
     keep = DevBuf<T>(count, s);
-    GPUPR_CUDA(cudaMemcpyAsync(keep.p, p, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    host_to_device(keep.p, p, count * sizeof(T), s);
     return keep.p;
 }
 
@@ -171,7 +164,7 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
 
     if (info.free_n == 0) {   // bindings.cpp:191-196: labels unchanged
         if (out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, d_labels, N, cudaMemcpyDeviceToDevice, s));
-        else GPUPR_CUDA(cudaMemcpyAsync(out, d_labels, N, cudaMemcpyDeviceToHost, s));
+        else device_to_host(out, d_labels, N, s);
         GPUPR_CUDA(cudaStreamSynchronize(s));
         st->kernel_launches = launches;
         st->native_total_seconds = seconds_since(all0);
@@ -193,7 +186,7 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
     }
     GPUPR_CUDA(cudaMemcpyAsync(d_out, d_labels, N, cudaMemcpyDeviceToDevice, s));
     scatter_partition(g.n, g.free_old.p, w.height.p, d_out, s, &launches);
-    if (!out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, d_out, N, cudaMemcpyDeviceToHost, s));
+    if (!out_dev) device_to_host(out, d_out, N, s);
     GPUPR_CUDA(cudaStreamSynchronize(s));
     st->partition_seconds = seconds_since(p0);
 
@@ -279,7 +272,7 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     st->free_n = info.free_n;
     if (info.free_n == 0) {
         if (out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, d_labels, N, cudaMemcpyDeviceToDevice, s));
-        else GPUPR_CUDA(cudaMemcpyAsync(out, d_labels, N, cudaMemcpyDeviceToHost, s));
+        else device_to_host(out, d_labels, N, s);
         GPUPR_CUDA(cudaStreamSynchronize(s));
         st->kernel_launches = launches;
         st->native_total_seconds = seconds_since(all0);
@@ -314,7 +307,7 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     batch_flows(G, d_foff.p, g.term.p, w.excess.p, g.base_node.p, raw.p, base.p, s, &launches);
     GPUPR_CUDA(cudaMemcpyAsync(hr.data(), raw.p, G * 8u, cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaMemcpyAsync(hb.data(), base.p, G * 8u, cudaMemcpyDeviceToHost, s));
-    if (!out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, d_out, N, cudaMemcpyDeviceToHost, s));
+    if (!out_dev) device_to_host(out, d_out, N, s);
     GPUPR_CUDA(cudaStreamSynchronize(s));
     for (uint32_t k = 0; k < G; ++k) {
         items[k].raw_flow = hr[k];
@@ -661,6 +654,22 @@ gpupr_status gpupr_solve_reduced_noalloc(uint32_t n, int32_t* d_neighbors, uint3
             stats->bfs_levels = sr.bfs_levels;
             stats->kernel_launches = sr.launches;
         }
+    });
+}
+
+gpupr_status gpupr_upload_topology(const void* host, uint64_t rows, int64_t row_stride_bytes,
+                                   int64_t col_stride_bytes, int32_t elem_bytes, int32_t* d_out,
+                                   void* stream)
+{
+    return guarded([&] {
+        if (!rows) return;
+        if (!host || !d_out) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL topology pointer"};
+        if (elem_bytes != 4 && elem_bytes != 8)
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "topology elements must be int32 or int64"};
+        if (!aligned(d_out, 16)) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "d_out must be 16-byte aligned"};
+        select_device_for(d_out, "d_out");
+        upload_topology(d_out, host, rows, row_stride_bytes, col_stride_bytes, elem_bytes,
+                        static_cast<cudaStream_t>(stream));
     });
 }
 

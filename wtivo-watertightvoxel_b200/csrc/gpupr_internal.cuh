@@ -108,6 +108,23 @@ struct DevBuf {
     size_t bytes() const { return n * sizeof(T); }
 };
 
+// Copies between pageable host arrays and the device through pinned staging
+// and a host copy pool (hostio.cu).  host_to_device returns once the host
+// array has been read (the device copy is ordered on s); device_to_host
+// returns once the host array holds the data.
+void host_to_device(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s);
+void device_to_host(void* h_dst, const void* d_src, size_t bytes, cudaStream_t s);
+void upload_topology(int32_t* d_out, const void* host, uint64_t rows, int64_t row_stride,
+                     int64_t col_stride, int elem_bytes, cudaStream_t s);
+
+// Per-thread cached host resources of the current device (hostio.cu): a
+// pinned mirror of the solver control block and timing events (slots 0-7;
+// 0-1 build timer, 2-5 solver).  A call creates and frees none of them, so
+// it never pays for pinning host pages, nor for the device-wide
+// synchronisation that freeing pinned memory implies.
+Ctl* pinned_ctl();
+cudaEvent_t timing_event(int slot);
+
 // Launch geometry: number of SMs of the current device (cached).
 int sm_count();
 

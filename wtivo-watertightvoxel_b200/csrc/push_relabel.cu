@@ -513,20 +513,14 @@ __global__ void k_bounded_wait(const volatile uint32_t* flag, unsigned long long
     }
 }
 
-struct PinnedCtl {
-    Ctl* h = nullptr;
-    PinnedCtl() { GPUPR_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h), sizeof(Ctl))); }
-    ~PinnedCtl() { if (h) cudaFreeHost(h); }
-};
-
-Ctl& read_ctl(PinnedCtl& pc, const Ctl* d, cudaStream_t s)
+Ctl& read_ctl(Ctl* h, const Ctl* d, cudaStream_t s)
 {
-    GPUPR_CUDA(cudaMemcpyAsync(pc.h, d, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaMemcpyAsync(h, d, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaStreamSynchronize(s));
-    if (pc.h->error)
-        throw Error{(gpupr_status)pc.h->error,
-                    "GPUPr-B200 device invariant failed code=" + std::to_string(pc.h->error)};
-    return *pc.h;
+    if (h->error)
+        throw Error{(gpupr_status)h->error,
+                    "GPUPr-B200 device invariant failed code=" + std::to_string(h->error)};
+    return *h;
 }
 
 }  // namespace
@@ -604,14 +598,8 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     p.limit_ns = (unsigned long long)(opt.time_limit_s * 1e9);
     p.wait_ns = 10ull * 1000ull * 1000ull * 1000ull;   // one step never takes this long
 
-    PinnedCtl pc;
-    cudaEvent_t e0, e1;
-    GPUPR_CUDA(cudaEventCreate(&e0));
-    GPUPR_CUDA(cudaEventCreate(&e1));
-    struct EvGuard {
-        cudaEvent_t a, b;
-        ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
-    } evg{e0, e1};
+    Ctl* pc = pinned_ctl();
+    cudaEvent_t e0 = timing_event(2), e1 = timing_event(3);
     const auto t0 = Clock::now();
     GPUPR_CUDA(cudaMemsetAsync(g.ctl, 0, sizeof(Ctl), s));
     GPUPR_CUDA(cudaEventRecord(e0, s));
@@ -620,9 +608,9 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     GPUPR_CUDA(cudaLaunchCooperativeKernel((const void*)k_solve_persistent, dim3(grid), dim3(DTPB),
                                            args, 0, s));
     GPUPR_CUDA(cudaEventRecord(e1, s));
-    GPUPR_CUDA(cudaMemcpyAsync(pc.h, g.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaMemcpyAsync(pc, g.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaStreamSynchronize(s));
-    const Ctl& hc = *pc.h;
+    const Ctl& hc = *pc;
     if (hc.error == (int)GPUPR_ERR_TIMEOUT)
         throw Error{GPUPR_ERR_TIMEOUT, "GPUPr-FAST-v6.30 solve exceeded 240s safety limit"};
     if (hc.error == (int)GPUPR_ERR_MAX_ROUNDS)
@@ -684,16 +672,8 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
     }
     out.engine = 1;
     const int grid = sm_count() * (opt.blocks_per_sm > 0 ? opt.blocks_per_sm : 4);
-    PinnedCtl pc;
-    cudaEvent_t e0, e1, ba, bb;
-    GPUPR_CUDA(cudaEventCreate(&e0));
-    GPUPR_CUDA(cudaEventCreate(&e1));
-    GPUPR_CUDA(cudaEventCreate(&ba));
-    GPUPR_CUDA(cudaEventCreate(&bb));
-    struct EvGuard {
-        cudaEvent_t a, b, c, d;
-        ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); cudaEventDestroy(d); }
-    } evg{e0, e1, ba, bb};
+    Ctl* pc = pinned_ctl();
+    cudaEvent_t e0 = timing_event(2), e1 = timing_event(3), ba = timing_event(4), bb = timing_event(5);
     // device time of one batch (the host waits for the batch anyway)
     auto batch_ms = [&]() {
         float ms = 0.f;
@@ -736,15 +716,15 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
                 throw Error{GPUPR_ERR_INVARIANT, "GPUPr-FAST-v6.30 BFS exceeded n+1 levels"};
         }
         ++out.relabels;
-        out.bfs_levels += pc.h->bfs_levels;
+        out.bfs_levels += pc->bfs_levels;
         last_bfs_s = std::chrono::duration<double>(Clock::now() - b0).count();
-        const uint32_t active = pc.h->act_cnt[0];
+        const uint32_t active = pc->act_cnt[0];
         if (active == 0) break;   // maximum preflow: no excess can reach the sink
         if (rounds_total >= opt.max_rounds)
             throw Error{GPUPR_ERR_MAX_ROUNDS, "GPUPr-FAST-v6.30 max macro rounds exceeded"};
 
         // ---- discharge rounds until idle, period or work budget ----
-        const unsigned long long visits0 = pc.h->node_visits;
+        const unsigned long long visits0 = pc->node_visits;
         uint32_t r = 0;
         for (;;) {
             uint64_t left = opt.max_rounds - rounds_total;
@@ -778,7 +758,7 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
     GPUPR_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
     GPUPR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    const Ctl& hc = *pc.h;
+    const Ctl& hc = *pc;
     out.raw_flow = (int64_t)hc.sink_flow;
     out.rounds = hc.rounds_done;
     out.node_visits = hc.node_visits;

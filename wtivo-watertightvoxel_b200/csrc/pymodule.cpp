@@ -170,6 +170,40 @@ py::tuple surface_extraction_topology_cuda(U8 labels, F64 vertices, py::object t
     return py::make_tuple(OV, OF);
 }
 
+// wtivo.py:284-309: Nx4 topology (any integer layout numpy accepts) -> one
+// contiguous int32 CUDA tensor on the current device, same shape check and
+// message; the copy goes through pinned staging with a parallel row gather
+// instead of 262k-row host repacks and blocking pageable copies.
+py::object topology_to_cuda_chunked(py::object host_array, const std::string& tag)
+{
+    py::module_ np = py::module_::import("numpy");
+    py::array a = np.attr("asarray")(host_array);
+    if (a.ndim() != 2 || a.shape(1) != 4)
+        throw std::runtime_error(tag + ": expected Nx4 topology array, got " +
+                                 std::string(py::str(a.attr("shape"))));
+    const char kind = a.dtype().kind();
+    const int item = (int)a.itemsize();
+    if (!((kind == 'i' || kind == 'u') && (item == 4 || item == 8)))
+        a = np.attr("asarray")(a, np.attr("int64"));
+    const int eb = (int)a.itemsize();
+    const std::uint64_t n = static_cast<std::uint64_t>(a.shape(0));
+    py::module_ torch = py::module_::import("torch");
+    py::object out = torch.attr("empty")(py::make_tuple(n, 4), py::arg("dtype") = torch.attr("int32"),
+                                         py::arg("device") = "cuda");
+    const int device = out.attr("device").attr("index").cast<int>();
+    void* stream = current_stream(device);
+    auto* dst = reinterpret_cast<std::int32_t*>(out.attr("data_ptr")().cast<uintptr_t>());
+    const void* src = a.data();
+    const std::int64_t rs = a.strides(0), cs = a.strides(1);
+    gpupr_status rc;
+    {
+        py::gil_scoped_release nogil;
+        rc = gpupr_upload_topology(src, n, rs, cs, eb, dst, stream);
+    }
+    if (rc != GPUPR_OK) raise_status(rc);
+    return out;
+}
+
 py::dict last_stats()
 {
     const gpupr_cut_stats& s = t_last;
@@ -214,6 +248,9 @@ PYBIND11_MODULE(wtivo_gpupr, m)
     m.def("surface_extraction_topology_cuda", &surface_extraction_topology_cuda, py::arg("labels"),
           py::arg("vertices"), py::arg("tets_cuda"), py::arg("neighbors_cuda"),
           py::arg("threads") = 16);
+    m.def("topology_to_cuda_chunked", &topology_to_cuda_chunked, py::arg("host_array"),
+          py::arg("tag") = "topology",
+          "Nx4 host topology -> contiguous int32 CUDA tensor (replaces wtivo.py's helper).");
     m.def("last_stats", &last_stats,
           "Extended statistics of the last graph_cut_fast call on this thread.");
     m.def("release_cached_memory", []() {

@@ -266,13 +266,13 @@ void surface_count(const uint8_t* labels, int l_dev, const double* vertices, uin
     const uint8_t* d_labels = labels;
     if (!l_dev && N) {
         dlab = DevBuf<uint8_t>(N, s);
-        GPUPR_CUDA(cudaMemcpyAsync(dlab.p, labels, N, cudaMemcpyHostToDevice, s));
+        host_to_device(dlab.p, labels, N, s);
         d_labels = dlab.p;
     }
     st->d_vertices = vertices;
     if (!v_dev && nv) {
         st->vcopy = DevBuf<double>(nv * 3u, s);
-        GPUPR_CUDA(cudaMemcpyAsync(st->vcopy.p, vertices, nv * 24u, cudaMemcpyHostToDevice, s));
+        host_to_device(st->vcopy.p, vertices, nv * 24u, s);
         st->d_vertices = st->vcopy.p;
     }
     uint64_t launches = 0;
@@ -330,13 +330,13 @@ void surface_fetch(int32_t* faces, double* verts, int out_dev, cudaStream_t s)
         if (!out_dev) { tmpf = DevBuf<int3>(st.faces, s); dfaces = tmpf.p; }
         k_surf_remap<<<grid_for(st.faces), TPB, 0, s>>>(st.faces, st.raw.p, st.remap.p, dfaces);
         GPUPR_CUDA(cudaGetLastError());
-        if (!out_dev) GPUPR_CUDA(cudaMemcpyAsync(faces, dfaces, st.faces * 12u, cudaMemcpyDeviceToHost, s));
+        if (!out_dev) device_to_host(faces, dfaces, st.faces * 12u, s);
         double* dverts = verts;
         DevBuf<double> tmpv;
         if (!out_dev) { tmpv = DevBuf<double>(st.used * 3u, s); dverts = tmpv.p; }
         k_vert_gather<<<grid_for(st.nv), TPB, 0, s>>>(st.nv, st.remap.p, st.d_vertices, dverts);
         GPUPR_CUDA(cudaGetLastError());
-        if (!out_dev) GPUPR_CUDA(cudaMemcpyAsync(verts, dverts, st.used * 24u, cudaMemcpyDeviceToHost, s));
+        if (!out_dev) device_to_host(verts, dverts, st.used * 24u, s);
         GPUPR_CUDA(cudaStreamSynchronize(s));
     }
     t_surf.reset();

@@ -64,8 +64,8 @@ class RequestResult(ctypes.Structure):
     _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int32), ("batch_size", ctypes.c_int32),
                 ("adjusted_flow", ctypes.c_int64), ("raw_flow", ctypes.c_int64),
                 ("n_tets", ctypes.c_uint64), ("free_n", ctypes.c_uint64),
-                ("queue_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
-                ("latency_ms", ctypes.c_double)]
+                ("queue_ms", ctypes.c_double), ("upload_ms", ctypes.c_double),
+                ("solve_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
 
 
 class GpuprError(RuntimeError):
@@ -117,11 +117,13 @@ def lib():
         L.gpupr_solve_reduced_noalloc.argtypes = [ctypes.c_uint32, p, p, p, p, i32, u64, i32, p, p]
         L.gpupr_graph_cut_batch.argtypes = [ctypes.c_uint32, p, p, p, ctypes.c_int, p, p, p,
                                             ctypes.c_int, f64, p, p, ctypes.c_int, p, p, p]
-        L.gpupr_server_create.argtypes = [ctypes.c_uint64, p, ctypes.POINTER(p)]
+        L.gpupr_server_create.argtypes = [ctypes.c_uint64, ctypes.c_uint32, p, ctypes.POINTER(p)]
         L.gpupr_server_submit.argtypes = [p, p, ctypes.c_uint64, p, p, p, ctypes.c_uint64, f64,
-                                          ctypes.POINTER(ctypes.c_uint64)]
-        L.gpupr_server_wait.argtypes = [p, ctypes.c_uint64, f64, p, p]
+                                          p, ctypes.POINTER(ctypes.c_uint64)]
+        L.gpupr_server_wait.argtypes = [p, ctypes.c_uint64, f64, p]
         L.gpupr_server_destroy.argtypes = [p]
+        L.gpupr_upload_topology.argtypes = [p, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64,
+                                            ctypes.c_int32, p, p]
         L.gpupr_release_cached_memory.argtypes = []
         L.gpupr_selftest_bounded_wait.argtypes = [ctypes.c_uint32, p]
         for name in header_functions():
@@ -244,41 +246,45 @@ class Server:
     """Continuous-batching cut server (gpupr_server_*): submit() host graphs
     at any time, wait() for each result."""
 
-    def __init__(self, hbm_budget_bytes=0, opts=None):
+    def __init__(self, hbm_budget_bytes=0, opts=None, max_batch=0):
         import torch
 
         torch.cuda.init()
         lib()
         self._h = ctypes.c_void_p()
-        check(_lib.gpupr_server_create(int(hbm_budget_bytes),
+        check(_lib.gpupr_server_create(int(hbm_budget_bytes), int(max_batch),
                                        ctypes.byref(opts) if opts is not None else None,
                                        ctypes.byref(self._h)))
-        self._n = {}
+        self._held = {}
 
     def submit(self, vertices, tets, nbrs, labels, fill_T=10.0):
+        """Queue one cut; the arrays are held (the server reads them in
+        place) until wait() returns for the request."""
         V = np.ascontiguousarray(vertices, np.float64)
         T = np.ascontiguousarray(tets, np.int32)
         Nb = np.ascontiguousarray(nbrs, np.int32)
         L = np.ascontiguousarray(labels, np.uint8)
+        out = np.empty(max(len(L), 1), np.uint8)
         rid = ctypes.c_uint64(0)
         check(_lib.gpupr_server_submit(self._h, _hp(V), len(V), _hp(T), _hp(Nb), _hp(L), len(L),
-                                       float(fill_T), ctypes.byref(rid)))
-        self._n[rid.value] = len(L)
+                                       float(fill_T), _hp(out), ctypes.byref(rid)))
+        self._held[rid.value] = (V, T, Nb, L, out)
         return rid.value
 
     def wait(self, rid, timeout_s=0.0):
-        out = np.empty(max(self._n[rid], 1), np.uint8)
         res = RequestResult()
-        rc = _lib.gpupr_server_wait(self._h, ctypes.c_uint64(rid), float(timeout_s), _hp(out),
-                                    ctypes.byref(res))
-        n = self._n.pop(rid)
+        rc = _lib.gpupr_server_wait(self._h, ctypes.c_uint64(rid), float(timeout_s), ctypes.byref(res))
+        if rc != 0 and res.id != rid:   # not finished (or unknown id): arrays stay held
+            check(rc)
+        held = self._held.pop(rid)
         check(rc)
-        return out[:n], {k: getattr(res, k) for k, _ in RequestResult._fields_}
+        return held[4][:len(held[3])], {k: getattr(res, k) for k, _ in RequestResult._fields_}
 
     def close(self):
         if self._h:
             _lib.gpupr_server_destroy(self._h)
             self._h = ctypes.c_void_p()
+            self._held.clear()
 
     def __enter__(self):
         return self
@@ -368,6 +374,17 @@ def bounded_wait_selftest(limit_us=200_000):
     import torch
 
     return lib().gpupr_selftest_bounded_wait(int(limit_us), _stream(torch))
+
+
+def upload_topology(host, out):
+    """gpupr_upload_topology: host Nx4 int32/int64 array (any strides) ->
+    the contiguous int32 CUDA tensor ``out``."""
+    import torch
+
+    a = np.asarray(host)
+    check(lib().gpupr_upload_topology(ctypes.c_void_p(a.ctypes.data), a.shape[0], a.strides[0],
+                                      a.strides[1], a.itemsize, _dp(out), _stream(torch, out.device)))
+    return out
 
 
 def release_cached_memory():
