@@ -81,15 +81,23 @@ typedef struct {
 /* Solver tuning knobs; zero fields take the defaults shown. */
 typedef struct {
     int32_t local_steps;          /* 1..32, default 8 */
-    int32_t global_relabel_period;/* old-equivalent rounds (default 1024) */
+    int32_t global_relabel_period;/* default 1024; one-launch-per-step engine:
+                                     relabel every ceil(period/local_steps)
+                                     rounds (gpu_push_relabel_fast.cu:476-480);
+                                     persistent engine: at most `period`
+                                     rounds between relabels; < 0 = no cap */
     uint64_t max_rounds;          /* default 2,000,000 */
     double time_limit_seconds;    /* default 240 */
     int32_t round_batch;          /* rounds enqueued per host check, default 24 */
     int32_t bfs_batch;            /* BFS levels enqueued per host check, default 48 */
     int32_t block_size;           /* threads per block, default 256 */
-    int32_t blocks_per_sm;        /* persistent grid multiplier, default 4 */
+    int32_t blocks_per_sm;        /* resident blocks per SM; default: 4 (one
+                                     launch per step), by graph size 1..4
+                                     (persistent) */
     double work_relabel_factor;   /* relabel after this many node visits per
-                                     free node since the last one (default 3) */
+                                     free node since the last one; default 3
+                                     (one launch per step), 2 below 500k free
+                                     nodes else 1 (persistent) */
     int32_t engine;               /* 0 auto (persistent when the device supports
                                      cooperative launch), 1 one launch per BFS
                                      level / round, 2 persistent */

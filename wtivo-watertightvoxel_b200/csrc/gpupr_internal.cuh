@@ -33,12 +33,15 @@ struct Ctl {
     unsigned long long pushes;
     unsigned long long bfs_visits;
     unsigned long long relabels;
-    uint32_t bar_arrive;     // persistent engine: grid barrier arrivals
-    uint32_t bar_gen;        // persistent engine: grid barrier generation
+    unsigned long long bar;  // persistent engine: barrier arrivals since launch
+                             // (low 40 bits) | BAR_ABORT once an error is raised
     uint32_t relabel_phases; // persistent engine: global relabels run
     uint32_t pad0;
     unsigned long long reserved[2];
 };
+
+constexpr unsigned long long BAR_ABORT = 1ull << 62;
+constexpr unsigned long long BAR_COUNT = (1ull << 40) - 1;
 
 // View of the reduced graph + solver workspace handed to kernels.
 struct SolveView {
@@ -196,13 +199,14 @@ void partition_from_height(uint32_t n, const uint32_t* d_height, uint8_t* d_part
 struct SolveOptions {
     int local_steps = 8;
     int relabel_rounds = 128;      // ceil(period / local_steps), 0 = only when idle
+    int period = 1024;             // global_relabel_period as given (clamped, 0 = none)
     uint64_t max_rounds = 2000000ull;
     double time_limit_s = 240.0;
     int round_batch = 24;
     int bfs_batch = 48;
     int block = 256;
-    int blocks_per_sm = 4;
-    double work_factor = 3.0;
+    int blocks_per_sm = 0;         // 0: by graph size (persistent), 4 (one launch per step)
+    double work_factor = 0.0;      // node visits per node between relabels, 0 = engine default
     int engine = 0;                // 0 auto, 1 one launch per step, 2 persistent
 };
 

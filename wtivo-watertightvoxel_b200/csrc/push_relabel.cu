@@ -57,6 +57,14 @@ __device__ __forceinline__ T warp_block_sum(T v, T* sh)
     return t;
 }
 
+// Records the first device error and makes every block waiting in (or later
+// reaching) a grid barrier of the persistent engine leave it.
+__device__ __forceinline__ void raise_error(Ctl* ctl, int code)
+{
+    atomicCAS(&ctl->error, 0, code);
+    atomicOr(&ctl->bar, BAR_ABORT);
+}
+
 // Copy a block's staged entries to a global queue of capacity cap.  Queue
 // entries are unique by construction (each node is appended at most once per
 // round or BFS); the guard keeps the writes inside the buffer even if that
@@ -64,8 +72,7 @@ __device__ __forceinline__ T warp_block_sum(T v, T* sh)
 __device__ __forceinline__ void flush_stage(const uint32_t* s_src, uint32_t count, uint32_t base,
                                             uint32_t* dst, uint32_t cap, Ctl* ctl)
 {
-    if (threadIdx.x == 0 && (uint64_t)base + count > cap)
-        atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_INVARIANT);
+    if (threadIdx.x == 0 && (uint64_t)base + count > cap) raise_error(ctl, (int)GPUPR_ERR_INVARIANT);
     for (uint32_t j = threadIdx.x; j < count; j += DTPB)
         if (base + j < cap) dst[base + j] = s_src[j];
 }
@@ -78,6 +85,9 @@ __global__ void __launch_bounds__(DTPB) k_init_excess(uint32_t n, const int32_t*
         excess[v] = t > 0 ? (long long)t : 0ll;   // source arc saturated (.cu:69-83)
     }
 }
+
+// Frontier size up to which a BFS level loads every neighbor's state at once.
+constexpr uint32_t BFS_EAGER_MAX = 32768u;
 
 // Level 1 of the backward BFS: nodes with a residual arc to the sink.  Every
 // other height is reset to UNVIS (.cu:374-379).  s_m[0..5] are the block's
@@ -122,6 +132,7 @@ __device__ __forceinline__ void bfs_level_body(const SolveView& g, uint32_t L, u
     uint32_t* out = (L & 1) ? g.fr[0] : g.fr[1];
     uint32_t* gcnt = &ctl->bfs_cnt[(L + 1) % 3];
     const uint32_t newh = L + 1u;
+    const bool eager = cnt <= BFS_EAGER_MAX;
     for (uint32_t base = blockIdx.x * DTPB; base < cnt; base += gridDim.x * DTPB) {
         const uint32_t i = base + threadIdx.x;
         if (i < cnt) {
@@ -130,16 +141,43 @@ __device__ __forceinline__ void bfs_level_body(const SolveView& g, uint32_t L, u
             const uint32_t rv = __ldg(g.rev + u);
             const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
             ++visits;
+            if (eager) {
+                // small frontier (latency bound): the neighbors' heights,
+                // reverse residuals and excesses are loaded at once, one
+                // round trip, then tested
+                uint32_t hv[4], rr[4];
+                long long xv[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int v = nb[k];
-                if (v < 0) continue;
-                if (ldcg(g.height + v) != UNVIS) continue;
-                const uint32_t rk = (rv >> (2 * k)) & 3u;
-                if (ldcg(g.res + (size_t)v * 4u + rk) == 0u) continue;
-                if (atomicCAS(g.height + v, UNVIS, newh) == UNVIS) {
-                    s_fr[atomicAdd(&s_m[0], 1u)] = (uint32_t)v;
-                    if (newh < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_m[1], 1u)] = (uint32_t)v;
+                for (int k = 0; k < 4; ++k) {
+                    const int v = nb[k] < 0 ? 0 : nb[k];
+                    const uint32_t rk = (rv >> (2 * k)) & 3u;
+                    hv[k] = ldcg(g.height + v);
+                    rr[k] = ldcg(g.res + (size_t)v * 4u + rk);
+                    xv[k] = ldcg(g.excess + v);
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int v = nb[k];
+                    if (v < 0 || hv[k] != UNVIS || rr[k] == 0u) continue;
+                    if (atomicCAS(g.height + v, UNVIS, newh) == UNVIS) {
+                        s_fr[atomicAdd(&s_m[0], 1u)] = (uint32_t)v;
+                        if (newh < g.n && xv[k] > 0) s_act[atomicAdd(&s_m[1], 1u)] = (uint32_t)v;
+                    }
+                }
+            } else {
+                // large frontier (traffic bound): most neighbors are already
+                // labeled, so a residual or excess is read only when needed
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int v = nb[k];
+                    if (v < 0) continue;
+                    if (ldcg(g.height + v) != UNVIS) continue;
+                    const uint32_t rk = (rv >> (2 * k)) & 3u;
+                    if (ldcg(g.res + (size_t)v * 4u + rk) == 0u) continue;
+                    if (atomicCAS(g.height + v, UNVIS, newh) == UNVIS) {
+                        s_fr[atomicAdd(&s_m[0], 1u)] = (uint32_t)v;
+                        if (newh < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_m[1], 1u)] = (uint32_t)v;
+                    }
                 }
             }
         }
@@ -200,14 +238,16 @@ __device__ __forceinline__ void discharge_node(const SolveView& g, uint32_t v, u
                                                uint32_t* s_cnt, Work& w)
 {
     const uint32_t n = g.n;
-    uint32_t h = ldcg(g.height + v);   // L2: a previous owner may have run on another SM
-    if (h >= n) return;
+    // every load of the node's own state is issued before any test, so they
+    // share one round trip to L2 (a queued node nearly always passes both
+    // tests); L2 loads because a previous owner may have run on another SM
+    uint32_t h = ldcg(g.height + v);
     long long ex = ldcg(g.excess + v);
-    if (ex <= 0) return;
     const int4 nb4 = __ldg(g.nbr + v);
     const uint4 r4 = __ldcg(reinterpret_cast<const uint4*>(g.res) + v);
     const uint32_t rv = __ldg(g.rev + v);
     int32_t t = ldcg(g.term + v);
+    if (h >= n || ex <= 0) return;
     const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
     uint32_t r[4] = {r4.x, r4.y, r4.z, r4.w};
     uint32_t hn[4];
@@ -288,7 +328,7 @@ __device__ __forceinline__ void discharge_body(const SolveView& g, uint32_t roun
         if (i < cnt) {
             const uint32_t v = __ldcg(in + i);
             if (v < g.n) discharge_node(g, v, s_buf, &s_m[0], w);
-            else atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_INVARIANT);
+            else raise_error(ctl, (int)GPUPR_ERR_INVARIANT);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -364,30 +404,51 @@ __device__ __forceinline__ unsigned long long gtimer()
 template <class T>
 __device__ __forceinline__ T vload(const T* p) { return *reinterpret_cast<const volatile T*>(p); }
 
-__device__ bool grid_barrier(Ctl* ctl, unsigned long long deadline, unsigned long long wait_ns,
-                             int* s_ok)
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void red_release_add(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid-wide barrier of the persistent engine (all blocks co-resident by the
+// cooperative launch).  ctl->bar counts arrivals since the launch; a block's
+// thread 0 adds its arrival with release semantics and polls with acquire
+// loads until the count reaches this barrier's target (kept per block in
+// `target`): one round trip to L2 to arrive, one to see the last arrival.
+// An error anywhere sets BAR_ABORT, which ends every wait at once; a wait
+// also ends, with GPUPR_ERR_TIMEOUT, after wait_ns, and block 0 raises the
+// solve's own time limit here.
+__device__ bool grid_barrier(Ctl* ctl, unsigned long long& target, unsigned long long deadline,
+                             unsigned long long wait_ns, int* s_ok)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned int gen = vload(&ctl->bar_gen);
-        __threadfence();
-        if (atomicAdd(&ctl->bar_arrive, 1u) == gridDim.x - 1) {
-            if (gtimer() > deadline) atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_TIMEOUT);
-            atomicExch(&ctl->bar_arrive, 0u);
-            __threadfence();
-            atomicAdd(&ctl->bar_gen, 1u);
-        } else {
-            const unsigned long long t0 = gtimer();
-            while (vload(&ctl->bar_gen) == gen) {
-                if (vload(&ctl->error)) break;
-                if (gtimer() - t0 > wait_ns) {
-                    atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_TIMEOUT);
+        target += gridDim.x;
+        if (blockIdx.x == 0 && gtimer() > deadline) raise_error(ctl, (int)GPUPR_ERR_TIMEOUT);
+        red_release_add(&ctl->bar, 1ull);
+        int ok = 1;
+        unsigned long long t0 = 0;
+        for (uint32_t it = 0;; ++it) {
+            const unsigned long long v = ld_acquire(&ctl->bar);
+            if (v & BAR_ABORT) { ok = 0; break; }
+            if ((v & BAR_COUNT) >= target) break;
+            if ((it & 63u) == 0u) {
+                const unsigned long long t = gtimer();
+                if (it == 0u) t0 = t;
+                else if (t - t0 > wait_ns) {
+                    raise_error(ctl, (int)GPUPR_ERR_TIMEOUT);
+                    ok = 0;
                     break;
                 }
             }
         }
-        __threadfence();
-        *s_ok = vload(&ctl->error) == 0;
+        *s_ok = ok;
     }
     __syncthreads();
     return *s_ok != 0;
@@ -402,6 +463,7 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
     Ctl* ctl = g.ctl;
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
     const unsigned long long deadline = gtimer() + p.limit_ns;
+    unsigned long long bar_target = 0;
     Work w;
     unsigned long long bfs_visits = 0;
     if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
@@ -409,25 +471,25 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
         const int32_t t = ldcg(g.term + v);
         g.excess[v] = t > 0 ? (long long)t : 0ll;   // source arc saturated (.cu:69-83)
     }
-    if (grid_barrier(ctl, deadline, p.wait_ns, &s_ok)) {
+    if (grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok)) {
         unsigned long long rounds_total = 0;
         uint32_t levels_total = 0, relabels = 0;
         bool ok = true;
         while (ok) {
             // ---- exact global relabel ----
             bfs_seed_body(g, s_buf, s_buf + DTPB * 4, s_m);
-            if (!(ok = grid_barrier(ctl, deadline, p.wait_ns, &s_ok))) break;
+            if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
             uint32_t L = 1;
             for (;;) {
                 const uint32_t cnt = min(vload(&ctl->bfs_cnt[L % 3]), g.n);
                 if (cnt == 0) break;
                 if (lead) ctl->bfs_cnt[(L + 2) % 3] = 0u;
                 bfs_level_body(g, L, cnt, s_buf, s_buf + DTPB * 4, s_m, bfs_visits);
-                if (!(ok = grid_barrier(ctl, deadline, p.wait_ns, &s_ok))) break;
+                if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
                 ++L;
                 ++levels_total;
                 if (L > g.n + 2u) {   // a BFS labels a new node per level
-                    if (lead) atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_INVARIANT);
+                    if (lead) raise_error(ctl, (int)GPUPR_ERR_INVARIANT);
                     ok = false;
                     break;
                 }
@@ -442,13 +504,13 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
                 const uint32_t cnt = min(vload(&ctl->act_cnt[r % 3]), g.n);
                 if (cnt == 0) break;
                 if (rounds_total >= p.max_rounds) {
-                    if (lead) atomicCAS(&ctl->error, 0, (int)GPUPR_ERR_MAX_ROUNDS);
+                    if (lead) raise_error(ctl, (int)GPUPR_ERR_MAX_ROUNDS);
                     ok = false;
                     break;
                 }
                 if (lead) ctl->act_cnt[(r + 2) % 3] = 0u;
                 discharge_body(g, r, cnt, s_buf, s_m, w);
-                if (!(ok = grid_barrier(ctl, deadline, p.wait_ns, &s_ok))) break;
+                if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
                 ++r;
                 ++rounds_total;
                 visits += cnt;
@@ -459,7 +521,7 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
             if (lead) {
                 for (int k = 0; k < 3; ++k) { ctl->act_cnt[k] = 0u; ctl->bfs_cnt[k] = 0u; }
             }
-            if (!(ok = grid_barrier(ctl, deadline, p.wait_ns, &s_ok))) break;
+            if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
         }
         if (lead) {
             ctl->rounds_done = (uint32_t)rounds_total;
@@ -565,6 +627,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
     if (!mr) mr = 2000000ull;
     r.local_steps = ls;
     r.relabel_rounds = period > 0 ? ((period + ls - 1) / ls < 1 ? 1 : (period + ls - 1) / ls) : 0;
+    r.period = period;
     r.max_rounds = mr;
     return r;
 }
@@ -588,12 +651,27 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     int bps = 0;
     GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent, DTPB, 0));
     if (bps < 1) throw Error{GPUPR_ERR_CUDA, "persistent solver kernel cannot be resident"};
-    const int want = opt.blocks_per_sm > 0 ? opt.blocks_per_sm : 4;
+    // resident blocks per SM: a step of a small graph is one chain of
+    // dependent L2 round trips plus a grid barrier whose cost grows with the
+    // number of blocks, while a large graph needs the threads to cover its
+    // frontiers (measured on B200: 1 is best below ~1.5M free nodes, 4 at
+    // ~77M)
+    const int want = opt.blocks_per_sm > 0 ? opt.blocks_per_sm
+                     : g.n < 1500000u     ? 1
+                     : g.n < 6000000u     ? 2
+                     : g.n < 40000000u    ? 3
+                                          : 4;
     const unsigned grid = (unsigned)(sm_count() * (want < bps ? want : bps));
     PersistParams p{};
     p.max_rounds = opt.max_rounds;
-    p.relabel_rounds = (uint32_t)(opt.relabel_rounds > 0 ? opt.relabel_rounds : 0);
-    const double budget = opt.work_factor > 0 ? opt.work_factor * (double)g.n : 0.0;
+    // Global relabels: a discharge phase ends once its node visits exceed
+    // work_factor x n (measured on B200: 2 suits graphs below ~500k free
+    // nodes, 1 larger ones), or after global_relabel_period rounds, a cap the
+    // work rule normally reaches first.  The result does not depend on this
+    // schedule: the solve always ends with an exact relabel.
+    p.relabel_rounds = (uint32_t)(opt.period > 0 ? opt.period : 0);
+    const double wf = opt.work_factor > 0 ? opt.work_factor : (g.n < 500000u ? 2.0 : 1.0);
+    const double budget = wf * (double)g.n;
     p.budget = budget > 1.8e19 ? 0ull : (unsigned long long)budget;
     p.limit_ns = (unsigned long long)(opt.time_limit_s * 1e9);
     p.wait_ns = 10ull * 1000ull * 1000ull * 1000ull;   // one step never takes this long
@@ -671,6 +749,7 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
         return;
     }
     out.engine = 1;
+    const double engine1_wf = opt.work_factor > 0 ? opt.work_factor : 3.0;
     const int grid = sm_count() * (opt.blocks_per_sm > 0 ? opt.blocks_per_sm : 4);
     Ctl* pc = pinned_ctl();
     cudaEvent_t e0 = timing_event(2), e1 = timing_event(3), ba = timing_event(4), bb = timing_event(5);
@@ -746,8 +825,7 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
             if (rounds_total >= opt.max_rounds)
                 throw Error{GPUPR_ERR_MAX_ROUNDS, "GPUPr-FAST-v6.30 max macro rounds exceeded"};
             if (opt.relabel_rounds > 0 && r >= (uint32_t)opt.relabel_rounds) break;
-            if (opt.work_factor > 0 &&
-                (double)(hc.node_visits - visits0) > opt.work_factor * (double)n)
+            if ((double)(hc.node_visits - visits0) > engine1_wf * (double)n)
                 break;
             const double el = std::chrono::duration<double>(Clock::now() - t0).count();
             if (el > opt.time_limit_s)
@@ -907,6 +985,7 @@ void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t*
     g.ctl = ctl;
     g.local_steps = opt.local_steps;
     const int grid = sm_count() * (opt.blocks_per_sm > 0 ? opt.blocks_per_sm : 4);
+    const double engine1_wf = opt.work_factor > 0 ? opt.work_factor : 3.0;
 
     Ctl hc{};
     // the array keeps the previous call's contents: the control block must
@@ -956,7 +1035,7 @@ void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t*
             if (rounds_total >= opt.max_rounds)
                 throw Error{GPUPR_ERR_MAX_ROUNDS, "GPUPr-FAST-v6.30 max macro rounds exceeded"};
             if (opt.relabel_rounds > 0 && r >= (uint32_t)opt.relabel_rounds) break;
-            if (opt.work_factor > 0 && (double)(hc.node_visits - visits0) > opt.work_factor * (double)n)
+            if ((double)(hc.node_visits - visits0) > engine1_wf * (double)n)
                 break;
             if (std::chrono::duration<double>(Clock::now() - t0).count() > opt.time_limit_s)
                 throw Error{GPUPR_ERR_TIMEOUT, "GPUPr-FAST-v6.30 solve exceeded 240s safety limit"};
