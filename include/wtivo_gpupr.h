@@ -324,6 +324,19 @@ gpupr_status gpupr_upload_topology(const void* host, uint64_t rows, int64_t row_
                                    int64_t col_stride_bytes, int32_t elem_bytes, int32_t* d_out,
                                    void* stream);
 
+/*
+ * Edge-degree watertight audit (replaces is_watertight,
+ * native/core/wtivo_core.cpp:402-464).  faces: n_faces x 3 int32 vertex ids,
+ * in host memory or, with faces_on_device, device memory (e.g. the output of
+ * gpupr_surface_fetch).  bad_groups = number of distinct undirected edges
+ * whose face count is not 2 (the mesh is watertight when n_faces > 0 and
+ * bad_groups == 0); table_bytes = device bytes of the edge table.  A
+ * negative vertex id fails with GPUPR_ERR_INVALID_ARGUMENT, "negative vertex
+ * index" (wtivo_core.cpp:424).
+ */
+gpupr_status gpupr_edge_audit(const int32_t* faces, uint64_t n_faces, int faces_on_device,
+                              uint64_t* bad_groups, uint64_t* table_bytes, void* stream);
+
 /* Release device memory cached between calls (pool + scratch). */
 gpupr_status gpupr_release_cached_memory(void);
 

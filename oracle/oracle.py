@@ -34,6 +34,7 @@ _ERRORS = {
     8: (MemoryError, "oracle out of host memory"),
     9: (RuntimeError, "GPUPr-FAST-v6.30 max macro rounds exceeded"),
     10: (RuntimeError, "device invariant failed: no residual out-arc"),
+    11: (RuntimeError, "negative vertex index"),
 }
 
 
@@ -88,9 +89,10 @@ def lib():
         L.orc_sink_reachable.argtypes = [ctypes.c_uint32, p, p, p, p]
         L.orc_graph_cut.argtypes = [p, u64, p, p, p, u64, f64, i32, p, p]
         L.orc_surface.argtypes = [p, p, u64, p, p, u64, p, p, p, p]
+        L.orc_edge_audit.argtypes = [p, u64, p]
         for name in ("orc_capacity", "orc_classify", "orc_build", "orc_reverse_slots",
                      "orc_maxflow_bk", "orc_maxflow_pr", "orc_sink_reachable",
-                     "orc_graph_cut", "orc_surface"):
+                     "orc_graph_cut", "orc_surface", "orc_edge_audit"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -240,3 +242,13 @@ def surface(labels, V, tets, nbrs):
                          labels.shape[0], ctypes.byref(nf), ctypes.byref(nu), _ptr(faces),
                          _ptr(verts)))
     return verts[: nu.value], faces[: nf.value]
+
+
+def edge_audit(faces):
+    """Edge-degree watertight audit (wtivo_core.cpp:402-464): returns the
+    number of bad edge groups (runs of equal undirected edges whose length
+    is not 2)."""
+    faces = _c(faces, np.int32).reshape(-1, 3)
+    bad = ctypes.c_uint64(0)
+    _check(lib().orc_edge_audit(_ptr(faces), faces.shape[0], ctypes.byref(bad)))
+    return int(bad.value)

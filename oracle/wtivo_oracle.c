@@ -743,3 +743,42 @@ int orc_surface(const uint8_t* lp, const double* V, uint64_t nv,
     free(remap);
     return ORC_OK;
 }
+
+static int cmp_u64(const void* a, const void* b)
+{
+    const uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+    return (x > y) - (x < y);
+}
+
+/* wtivo_core.cpp:418-447: edge keys, sort, runs of equal keys */
+int orc_edge_audit(const int32_t* faces, uint64_t nf, uint64_t* bad_groups)
+{
+    if (!bad_groups || (nf && !faces)) return ORC_ERR_ARG;
+    *bad_groups = 0;
+    if (nf == 0) return ORC_OK;
+    uint64_t* e = (uint64_t*)malloc(sizeof(uint64_t) * 3u * nf);
+    if (!e) return ORC_ERR_NO_MEM;
+    for (uint64_t i = 0; i < nf; ++i) {
+        const int32_t a = faces[3u * i], b = faces[3u * i + 1u], c = faces[3u * i + 2u];
+        if (a < 0 || b < 0 || c < 0) {
+            free(e);
+            return ORC_ERR_NEG_VERTEX;
+        }
+        const uint32_t ua = (uint32_t)a, ub = (uint32_t)b, uc = (uint32_t)c;
+        e[3u * i] = ((uint64_t)(ua < ub ? ua : ub) << 32) | (ua < ub ? ub : ua);
+        e[3u * i + 1u] = ((uint64_t)(ub < uc ? ub : uc) << 32) | (ub < uc ? uc : ub);
+        e[3u * i + 2u] = ((uint64_t)(uc < ua ? uc : ua) << 32) | (uc < ua ? ua : uc);
+    }
+    qsort(e, 3u * nf, sizeof(uint64_t), cmp_u64);
+    uint64_t bad = 0, p = 0;
+    const uint64_t m = 3u * nf;
+    while (p < m) {
+        uint64_t q = p + 1u;
+        while (q < m && e[q] == e[p]) ++q;
+        if (q - p != 2u) ++bad;
+        p = q;
+    }
+    free(e);
+    *bad_groups = bad;
+    return ORC_OK;
+}

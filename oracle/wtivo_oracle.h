@@ -44,7 +44,8 @@ enum {
     ORC_ERR_NO_REVERSE = 7,   /* asymmetric adjacency: reverse slot missing */
     ORC_ERR_NO_MEM = 8,
     ORC_ERR_MAX_ROUNDS = 9,
-    ORC_ERR_INVARIANT = 10    /* active node without residual out-arc */
+    ORC_ERR_INVARIANT = 10,   /* active node without residual out-arc */
+    ORC_ERR_NEG_VERTEX = 11   /* "negative vertex index" (wtivo_core.cpp:424) */
 };
 
 typedef struct {
@@ -123,6 +124,13 @@ int orc_surface(const uint8_t* labels, const double* V, uint64_t nv,
                 const int32_t* tets, const int32_t* nbrs, uint64_t N,
                 uint64_t* n_faces, uint64_t* n_used,
                 int32_t* out_faces, double* out_verts);
+
+/* Edge-degree watertight audit (native/core/wtivo_core.cpp:402-464): every
+ * face contributes its three undirected edges as keys (min << 32 | max),
+ * the keys are sorted, and each run of equal keys whose length is not 2 is
+ * one bad edge group.  A closed 2-manifold mesh has none.  Returns ORC_OK or
+ * ORC_ERR_NEG_VERTEX. */
+int orc_edge_audit(const int32_t* faces, uint64_t nf, uint64_t* bad_groups);
 
 #ifdef __cplusplus
 }

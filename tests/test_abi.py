@@ -103,3 +103,14 @@ def test_topology_upload_shape_check(built):
         wtivo_gpupr.topology_to_cuda_chunked(np.zeros((5, 3), np.int32), "tets")
     with pytest.raises(RuntimeError, match=r"nb: expected Nx4 topology array, got \(8,\)"):
         wtivo_gpupr.topology_to_cuda_chunked(np.zeros(8, np.int64), "nb")
+
+
+def test_is_watertight_checks_before_the_gpu(built):
+    """wtivo_core.cpp:408-413: shape check and the empty-mesh answer."""
+    import wtivo_gpupr
+
+    with pytest.raises(RuntimeError, match="is_watertight expects Fx3 int32 faces"):
+        wtivo_gpupr.is_watertight(np.zeros((5, 2), np.int32), 4)
+    with pytest.raises(RuntimeError, match="is_watertight expects Fx3 int32 faces"):
+        wtivo_gpupr.is_watertight(np.zeros(9, np.int32))
+    assert wtivo_gpupr.is_watertight(np.zeros((0, 3), np.int32), 16) == (False, 0, 0.0, 0)

@@ -192,3 +192,44 @@ def test_surface_oracle_matches_numpy():
     e = np.sort(np.concatenate([F1[:, [0, 1]], F1[:, [1, 2]], F1[:, [2, 0]]]), axis=1)
     _, cnt = np.unique(e, axis=0, return_counts=True)
     assert np.all(cnt % 2 == 0)
+
+
+def _numpy_bad_groups(F):
+    """Independent count for the audit: distinct undirected edges whose
+    multiplicity is not 2 (numpy unique over packed edge keys)."""
+    F = np.asarray(F, np.int64)
+    e = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]])
+    key = (np.minimum(e[:, 0], e[:, 1]) << 32) | np.maximum(e[:, 0], e[:, 1])
+    _, cnt = np.unique(key, return_counts=True)
+    return int((cnt != 2).sum())
+
+
+def audit_cases():
+    """Meshes with known edge defects (wtivo_core.cpp:402-464 semantics)."""
+    import synth
+
+    rng = np.random.default_rng(7)
+    V, F = synth.icosphere(3)
+    tet = np.array([[0, 1, 2], [0, 3, 1], [1, 3, 2], [2, 3, 0]], np.int32)
+    soup = rng.integers(0, 50, size=(400, 3)).astype(np.int32)
+    return {
+        "closed_icosphere": (F, 0),
+        "closed_tetrahedron": (tet, 0),
+        "one_face_missing": (F[1:], 3),
+        "duplicated_face": (np.concatenate([F, F[:1]]), 3),
+        "fin_on_an_edge": (np.concatenate([tet, [[0, 1, 4]]]).astype(np.int32), 3),
+        "holed": (synth.holed_icosphere(3, subdiv=3, frac=0.05)[1], None),
+        "soup": (soup, None),
+        "degenerate_face": (np.array([[0, 0, 1]], np.int32), None),
+    }
+
+
+def test_edge_audit_oracle_matches_numpy():
+    for name, (F, want) in audit_cases().items():
+        got = orc.edge_audit(F)
+        assert got == _numpy_bad_groups(F), name
+        if want is not None:
+            assert got == want, name
+    assert orc.edge_audit(np.zeros((0, 3), np.int32)) == 0
+    with pytest.raises(RuntimeError, match="negative vertex index"):
+        orc.edge_audit(np.array([[0, 1, -1]], np.int32))

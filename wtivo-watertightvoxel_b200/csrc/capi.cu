@@ -673,6 +673,23 @@ gpupr_status gpupr_upload_topology(const void* host, uint64_t rows, int64_t row_
     });
 }
 
+gpupr_status gpupr_edge_audit(const int32_t* faces, uint64_t n_faces, int faces_on_device,
+                              uint64_t* bad_groups, uint64_t* table_bytes, void* stream)
+{
+    return guarded([&] {
+        if (!bad_groups || !table_bytes) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL result pointer"};
+        *bad_groups = 0;
+        *table_bytes = 0;
+        if (!n_faces) return;
+        if (!faces) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "faces pointer is NULL"};
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (faces_on_device) select_device_for(faces, "faces");
+        DevBuf<int32_t> dfaces;
+        const int32_t* d = on_device(faces, n_faces * 3u, faces_on_device, dfaces, s);
+        edge_audit(d, n_faces, s, bad_groups, table_bytes, nullptr);
+    });
+}
+
 gpupr_status gpupr_release_cached_memory(void)
 {
     return guarded([&] {

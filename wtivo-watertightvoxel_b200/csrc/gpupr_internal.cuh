@@ -249,6 +249,12 @@ void surface_count(const uint8_t* labels, int l_dev, const double* vertices, uin
                    uint64_t* n_used, cudaStream_t s);
 void surface_fetch(int32_t* faces, double* verts, int out_dev, cudaStream_t s);
 
+// Edge-degree watertight audit of F device faces (audit.cu): the number of
+// distinct undirected edges whose face count is not 2, and the bytes of the
+// device edge table used.
+void edge_audit(const int32_t* d_faces, uint64_t nf, cudaStream_t s, uint64_t* bad_groups,
+                uint64_t* table_bytes, uint64_t* launches);
+
 // Allocation-free solve (push_relabel.cu): all scratch in a static device
 // array sized for NOALLOC_MAX_NODES nodes; the partition goes to d_partition.
 constexpr uint32_t NOALLOC_MAX_NODES = 1u << 20;

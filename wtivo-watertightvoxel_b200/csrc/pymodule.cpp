@@ -16,6 +16,7 @@
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 
+#include <chrono>
 #include <cstdint>
 #include <cstdlib>
 #include <iostream>
@@ -204,6 +205,55 @@ py::object topology_to_cuda_chunked(py::object host_array, const std::string& ta
     return out;
 }
 
+// native/core/wtivo_core.cpp:402-464 (is_watertight): same argument check,
+// message and 4-tuple (watertight, bad edge groups, seconds, edge buffer
+// bytes; the last is this implementation's device edge table).  faces may
+// also be a CUDA int32 Fx3 tensor, audited in place.
+py::tuple is_watertight(py::object faces, int threads)
+{
+    (void)threads;
+    const auto t0 = std::chrono::steady_clock::now();
+    const char* msg = "is_watertight expects Fx3 int32 faces";
+    py::module_ torch = py::module_::import("torch");
+    const int32_t* ptr = nullptr;
+    std::uint64_t nf = 0;
+    int on_device = 0;
+    void* stream = nullptr;
+    py::object keep;
+    if (py::isinstance(faces, torch.attr("Tensor")) && faces.attr("is_cuda").cast<bool>()) {
+        if (!py::object(faces.attr("dtype")).equal(torch.attr("int32")) ||
+            faces.attr("dim")().cast<int64_t>() != 2 || faces.attr("size")(1).cast<int64_t>() != 3 ||
+            !faces.attr("is_contiguous")().cast<bool>())
+            throw std::runtime_error(msg);
+        nf = faces.attr("size")(0).cast<std::uint64_t>();
+        ptr = reinterpret_cast<const int32_t*>(faces.attr("data_ptr")().cast<uintptr_t>());
+        on_device = 1;
+        stream = current_stream(faces.attr("device").attr("index").cast<int>());
+        keep = faces;
+    } else {
+        py::array_t<std::int32_t, py::array::c_style | py::array::forcecast> a =
+            py::array_t<std::int32_t, py::array::c_style | py::array::forcecast>::ensure(faces);
+        if (!a || a.ndim() != 2 || a.shape(1) != 3) throw std::runtime_error(msg);
+        nf = static_cast<std::uint64_t>(a.shape(0));
+        ptr = a.data();
+        keep = a;
+        if (nf) stream = current_stream(torch.attr("cuda").attr("current_device")().cast<int>());
+    }
+    if (nf == 0) return py::make_tuple(false, py::int_(0), py::float_(0.0), py::int_(0));
+    std::uint64_t bad = 0, bytes = 0;
+    gpupr_status rc;
+    {
+        py::gil_scoped_release nogil;
+        rc = gpupr_edge_audit(ptr, nf, on_device, &bad, &bytes, stream);
+    }
+    if (rc != GPUPR_OK) raise_status(rc);
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (verbose())
+        std::cout << "[WTiVo-Watertight] faces=" << nf << " | bad-edge-groups=" << bad
+                  << " | total=" << sec << "s" << std::endl;
+    return py::make_tuple(py::bool_(bad == 0), py::int_(bad), py::float_(sec), py::int_(bytes));
+}
+
 py::dict last_stats()
 {
     const gpupr_cut_stats& s = t_last;
@@ -248,6 +298,8 @@ PYBIND11_MODULE(wtivo_gpupr, m)
     m.def("surface_extraction_topology_cuda", &surface_extraction_topology_cuda, py::arg("labels"),
           py::arg("vertices"), py::arg("tets_cuda"), py::arg("neighbors_cuda"),
           py::arg("threads") = 16);
+    m.def("is_watertight", &is_watertight, py::arg("faces"), py::arg("threads") = 0,
+          "Edge-degree watertight audit on the GPU (replaces wtivo_core.is_watertight).");
     m.def("topology_to_cuda_chunked", &topology_to_cuda_chunked, py::arg("host_array"),
           py::arg("tag") = "topology",
           "Nx4 host topology -> contiguous int32 CUDA tensor (replaces wtivo.py's helper).");

@@ -124,6 +124,8 @@ def lib():
         L.gpupr_server_destroy.argtypes = [p]
         L.gpupr_upload_topology.argtypes = [p, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64,
                                             ctypes.c_int32, p, p]
+        L.gpupr_edge_audit.argtypes = [p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
+                                       ctypes.POINTER(ctypes.c_uint64), p]
         L.gpupr_release_cached_memory.argtypes = []
         L.gpupr_selftest_bounded_wait.argtypes = [ctypes.c_uint32, p]
         for name in header_functions():
@@ -385,6 +387,23 @@ def upload_topology(host, out):
     check(lib().gpupr_upload_topology(ctypes.c_void_p(a.ctypes.data), a.shape[0], a.strides[0],
                                       a.strides[1], a.itemsize, _dp(out), _stream(torch, out.device)))
     return out
+
+
+def edge_audit(faces):
+    """gpupr_edge_audit: faces numpy Fx3 (host) or CUDA int32 tensor.
+    Returns (bad_groups, table_bytes)."""
+    import torch
+
+    bad = ctypes.c_uint64(0)
+    nbytes = ctypes.c_uint64(0)
+    if isinstance(faces, torch.Tensor):
+        check(lib().gpupr_edge_audit(_dp(faces), faces.shape[0], 1, ctypes.byref(bad), ctypes.byref(nbytes),
+                                     _stream(torch, faces.device)))
+    else:
+        f = np.ascontiguousarray(faces, np.int32).reshape(-1, 3)
+        check(lib().gpupr_edge_audit(_hp(f), f.shape[0], 0, ctypes.byref(bad), ctypes.byref(nbytes),
+                                     _stream(torch)))
+    return int(bad.value), int(nbytes.value)
 
 
 def release_cached_memory():
