@@ -337,6 +337,48 @@ gpupr_status gpupr_upload_topology(const void* host, uint64_t rows, int64_t row_
 gpupr_status gpupr_edge_audit(const int32_t* faces, uint64_t n_faces, int faces_on_device,
                               uint64_t* bad_groups, uint64_t* table_bytes, void* stream);
 
+/*
+ * Sparse unsigned distance grid, the input of the tet-centroid label sampler
+ * (stands in for the reference's OpenVDB FloatGrid, native/vdb/wtivo_vdb.cpp:
+ * 1007-1070, built with a linear transform of voxel_size): voxel (i,j,k)
+ * sits at world (i,j,k) * voxel_size; bricks of 8^3 voxels; brick
+ * (bx,by,bz) of a dims[0] x dims[1] x dims[2] box holds voxels
+ * origin + 8*(bx,by,bz) + [0,8)^3.  table[(bx*dims[1] + by)*dims[2] + bz] is
+ * the brick's number in values (-1: every voxel of it is the background);
+ * values[brick*512 + (x*8 + y)*8 + z].  Voxels outside the box read the
+ * background.  table/values live in device memory when on_device, else in
+ * host memory (copied for the call).
+ */
+typedef struct {
+    double voxel_size;
+    int32_t origin[3];
+    int32_t dims[3];
+    float background;
+    int32_t on_device;
+    const int32_t* table;
+    const float* values;
+    uint64_t n_bricks;
+} gpupr_brick_grid;
+
+/*
+ * Tet-centroid labels (replaces SparseUDF.sample_tet_labels,
+ * native/vdb/wtivo_vdb.cpp:1519-1584): centroid = 0.25 * sum of the tet's 4
+ * vertices, mapped to ((c - bbox_min)/(bbox_max - bbox_min))*(1 - 2 padding)
+ * + padding, sampled with OpenVDB's BoxSampler semantics (trilinear over the
+ * 8 voxels around floor(index), index = world / voxel_size); labels_out[i] =
+ * 0 where the sample <= threshold, else 1.  tets (16-byte aligned when on the
+ * device), vertices, labels_out and udf_out (optional: the samples) each in
+ * host or device memory as flagged (udf_out follows labels_out).  Errors:
+ * "SparseUDF.sample_tet_labels: degenerate bbox", "... tet index out of
+ * range" (GPUPR_ERR_INVALID_ARGUMENT).
+ */
+gpupr_status gpupr_sample_tet_labels(const gpupr_brick_grid* grid, const double* vertices,
+                                     uint64_t n_vertices, int vertices_on_device,
+                                     const int32_t* tets, uint64_t n_tets, int tets_on_device,
+                                     const double* bbox_min, const double* bbox_max,
+                                     double padding, double threshold, uint8_t* labels_out,
+                                     int labels_on_device, float* udf_out, void* stream);
+
 /* Release device memory cached between calls (pool + scratch). */
 gpupr_status gpupr_release_cached_memory(void);
 

@@ -35,6 +35,8 @@ _ERRORS = {
     9: (RuntimeError, "GPUPr-FAST-v6.30 max macro rounds exceeded"),
     10: (RuntimeError, "device invariant failed: no residual out-arc"),
     11: (RuntimeError, "negative vertex index"),
+    12: (RuntimeError, "SparseUDF.sample_tet_labels: degenerate bbox"),
+    13: (RuntimeError, "SparseUDF.sample_tet_labels: tet index out of range"),
 }
 
 
@@ -90,9 +92,11 @@ def lib():
         L.orc_graph_cut.argtypes = [p, u64, p, p, p, u64, f64, i32, p, p]
         L.orc_surface.argtypes = [p, p, u64, p, p, u64, p, p, p, p]
         L.orc_edge_audit.argtypes = [p, u64, p]
+        L.orc_sample_tet_labels.argtypes = [p, p, u64, p, u64, p, p, f64, f64, p, p]
         for name in ("orc_capacity", "orc_classify", "orc_build", "orc_reverse_slots",
                      "orc_maxflow_bk", "orc_maxflow_pr", "orc_sink_reachable",
-                     "orc_graph_cut", "orc_surface", "orc_edge_audit"):
+                     "orc_graph_cut", "orc_surface", "orc_edge_audit",
+                     "orc_sample_tet_labels"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -252,3 +256,29 @@ def edge_audit(faces):
     bad = ctypes.c_uint64(0)
     _check(lib().orc_edge_audit(_ptr(faces), faces.shape[0], ctypes.byref(bad)))
     return int(bad.value)
+
+
+class BrickGrid(ctypes.Structure):
+    _fields_ = [("voxel_size", ctypes.c_double), ("origin", ctypes.c_int32 * 3),
+                ("dims", ctypes.c_int32 * 3), ("background", ctypes.c_float),
+                ("table", ctypes.c_void_p), ("values", ctypes.c_void_p)]
+
+
+def sample_tet_labels(grid, V, tets, bbox_min, bbox_max, padding, threshold):
+    """Tet-centroid labels (wtivo_vdb.cpp:1519-1584) on a brick grid (dict
+    as made by synth.brick_udf): returns (labels uint8[N], samples f32[N])."""
+    table = _c(grid["table"], np.int32).reshape(-1)
+    values = _c(grid["values"], np.float32).reshape(-1)
+    g = BrickGrid(float(grid["voxel_size"]), (ctypes.c_int32 * 3)(*[int(x) for x in grid["origin"]]),
+                  (ctypes.c_int32 * 3)(*[int(x) for x in grid["dims"]]), float(grid["background"]),
+                  table.ctypes.data, values.ctypes.data)
+    V = _c(V, np.float64)
+    tets = _c(tets, np.int32)
+    bmin = _c(bbox_min, np.float64)
+    bmax = _c(bbox_max, np.float64)
+    out = np.empty(max(len(tets), 1), np.uint8)
+    udf = np.empty(max(len(tets), 1), np.float32)
+    _check(lib().orc_sample_tet_labels(ctypes.byref(g), _ptr(V), V.shape[0], _ptr(tets), tets.shape[0],
+                                       _ptr(bmin), _ptr(bmax), float(padding), float(threshold),
+                                       _ptr(out), _ptr(udf)))
+    return out[:len(tets)], udf[:len(tets)]

@@ -782,3 +782,71 @@ int orc_edge_audit(const int32_t* faces, uint64_t nf, uint64_t* bad_groups)
     *bad_groups = bad;
     return ORC_OK;
 }
+
+/* value of voxel (i,j,k): background outside the brick box or in an
+ * inactive brick */
+static float grid_value(const orc_brick_grid* g, int64_t i, int64_t j, int64_t k)
+{
+    i -= g->origin[0];
+    j -= g->origin[1];
+    k -= g->origin[2];
+    if (i < 0 || j < 0 || k < 0) return g->background;
+    const int64_t bx = i >> 3, by = j >> 3, bz = k >> 3;
+    if (bx >= g->dims[0] || by >= g->dims[1] || bz >= g->dims[2]) return g->background;
+    const int32_t b = g->table[(bx * g->dims[1] + by) * g->dims[2] + bz];
+    if (b < 0) return g->background;
+    return g->values[(size_t)b * 512u + (size_t)(((i & 7) * 8 + (j & 7)) * 8 + (k & 7))];
+}
+
+/* one lerp of BoxSampler::trilinearInterpolation: a + float((b - a) * w) */
+static float box_lerp(float a, float b, double w)
+{
+    const float diff = b - a;
+    const double temp = (double)diff * w;
+    return a + (float)temp;
+}
+
+int orc_sample_tet_labels(const orc_brick_grid* g, const double* V, uint64_t nv,
+                          const int32_t* tets, uint64_t nt, const double* bmin,
+                          const double* bmax, double padding, double threshold,
+                          uint8_t* labels, float* udf)
+{
+    if (!g || !bmin || !bmax || (nt && (!V || !tets || !labels)) || !(g->voxel_size > 0.0))
+        return ORC_ERR_ARG;
+    const double sx = bmax[0] - bmin[0], sy = bmax[1] - bmin[1], sz = bmax[2] - bmin[2];
+    if (!(sx > 0 && sy > 0 && sz > 0)) return ORC_ERR_BBOX;         /* :1546-1547 */
+    const double scale = 1.0 - 2.0 * padding;
+    const double inv_h = 1.0 / g->voxel_size;   /* linear transform: index = world * (1/h) */
+    for (uint64_t i = 0; i < nt; ++i) {
+        double cx = 0.0, cy = 0.0, cz = 0.0;
+        for (int q = 0; q < 4; ++q) {                               /* :1563-1570 */
+            const int32_t vi = tets[4u * i + (uint64_t)q];
+            if (vi < 0 || (uint64_t)vi >= nv) return ORC_ERR_TET_INDEX;
+            cx += V[3u * (uint64_t)vi + 0u];
+            cy += V[3u * (uint64_t)vi + 1u];
+            cz += V[3u * (uint64_t)vi + 2u];
+        }
+        cx *= 0.25;
+        cy *= 0.25;
+        cz *= 0.25;
+        const double nx = ((cx - bmin[0]) / sx) * scale + padding;  /* :1572-1574 */
+        const double ny = ((cy - bmin[1]) / sy) * scale + padding;
+        const double nz = ((cz - bmin[2]) / sz) * scale + padding;
+        const double x = nx * inv_h, y = ny * inv_h, z = nz * inv_h;
+        const double fx = floor(x), fy = floor(y), fz = floor(z);
+        const int64_t ix = (int64_t)fx, iy = (int64_t)fy, iz = (int64_t)fz;
+        const double u = x - fx, v = y - fy, w = z - fz;
+        float d[2][2][2];
+        for (int a = 0; a < 2; ++a)
+            for (int b = 0; b < 2; ++b)
+                for (int c = 0; c < 2; ++c) d[a][b][c] = grid_value(g, ix + a, iy + b, iz + c);
+        const float val = box_lerp(box_lerp(box_lerp(d[0][0][0], d[0][0][1], w),
+                                            box_lerp(d[0][1][0], d[0][1][1], w), v),
+                                   box_lerp(box_lerp(d[1][0][0], d[1][0][1], w),
+                                            box_lerp(d[1][1][0], d[1][1][1], w), v),
+                                   u);
+        labels[i] = ((double)val <= threshold) ? 0u : 1u;             /* :1576 */
+        if (udf) udf[i] = val;
+    }
+    return ORC_OK;
+}

@@ -45,7 +45,9 @@ enum {
     ORC_ERR_NO_MEM = 8,
     ORC_ERR_MAX_ROUNDS = 9,
     ORC_ERR_INVARIANT = 10,   /* active node without residual out-arc */
-    ORC_ERR_NEG_VERTEX = 11   /* "negative vertex index" (wtivo_core.cpp:424) */
+    ORC_ERR_NEG_VERTEX = 11,  /* "negative vertex index" (wtivo_core.cpp:424) */
+    ORC_ERR_BBOX = 12,        /* "...sample_tet_labels: degenerate bbox" (wtivo_vdb.cpp:1547) */
+    ORC_ERR_TET_INDEX = 13    /* "...sample_tet_labels: tet index out of range" (:1566) */
 };
 
 typedef struct {
@@ -131,6 +133,33 @@ int orc_surface(const uint8_t* labels, const double* V, uint64_t nv,
  * one bad edge group.  A closed 2-manifold mesh has none.  Returns ORC_OK or
  * ORC_ERR_NEG_VERTEX. */
 int orc_edge_audit(const int32_t* faces, uint64_t nf, uint64_t* bad_groups);
+
+/* Sparse unsigned distance grid of 8^3-voxel bricks (host arrays): voxel
+ * (i,j,k) sits at world (i,j,k)*voxel_size; brick (bx,by,bz) of the box
+ * holds voxels origin + 8*(bx,by,bz) + [0,8)^3; table[(bx*dims[1]+by)*dims[2]+bz]
+ * is the brick's number in values (-1: every voxel = background);
+ * values[brick*512 + (x*8+y)*8+z]. */
+typedef struct {
+    double voxel_size;
+    int32_t origin[3];
+    int32_t dims[3];
+    float background;
+    const int32_t* table;
+    const float* values;
+} orc_brick_grid;
+
+/* Tet-centroid labels (native/vdb/wtivo_vdb.cpp:1519-1584,
+ * SparseUDF.sample_tet_labels): centroid = 0.25 * sum of the 4 vertices,
+ * mapped into the query box n = ((c - bmin)/(bmax - bmin))*(1 - 2 padding)
+ * + padding, to index space by the grid's linear transform (n * (1/h)),
+ * sampled by OpenVDB 12.0.1's BoxSampler (trilinear over the 8 voxels
+ * around floor(index): lerp along z, then y, then x, each lerp
+ * a + float((b - a) * w)); label 0 where the sample <= threshold, else 1.
+ * udf (optional) receives the samples. */
+int orc_sample_tet_labels(const orc_brick_grid* g, const double* V, uint64_t nv,
+                          const int32_t* tets, uint64_t nt, const double* bmin,
+                          const double* bmax, double padding, double threshold,
+                          uint8_t* labels, float* udf);
 
 #ifdef __cplusplus
 }

@@ -233,3 +233,68 @@ def test_edge_audit_oracle_matches_numpy():
     assert orc.edge_audit(np.zeros((0, 3), np.int32)) == 0
     with pytest.raises(RuntimeError, match="negative vertex index"):
         orc.edge_audit(np.array([[0, 1, -1]], np.int32))
+
+
+def label_case(n_cubes=40, seed=0, h=1.0 / 128):
+    """A sphere-mesh UDF brick grid in the unit query box and a jittered
+    lattice of tets over it (the label sampler's inputs)."""
+    import synth
+
+    V, F = synth.icosphere(4, 0.3, (0.5, 0.5, 0.5))
+    grid = synth.brick_udf(V, F, h, 3.0)
+    TV, T, _ = synth.lattice_cells((n_cubes,) * 3, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), seed=seed)
+    return V, F, grid, TV, T
+
+
+def test_label_sampler_oracle_is_the_box_sampler():
+    """On a field linear in the voxel index the box sampler is exact; on a
+    mesh UDF the sample tracks the exact distance within a voxel."""
+    import synth
+
+    V, F, grid, TV, T = label_case()
+    lin = dict(grid)
+    tab = grid["table"]
+    idx = np.argwhere(tab >= 0)
+    vals = np.empty_like(grid["values"])
+    l = np.arange(8)
+    for b, (bx, by, bz) in zip(tab[tuple(idx.T)], idx):
+        i = grid["origin"][0] + 8 * bx + l[:, None, None]
+        j = grid["origin"][1] + 8 * by + l[None, :, None]
+        k = grid["origin"][2] + 8 * bz + l[None, None, :]
+        vals[b] = (0.001 * i + 0.002 * j + 0.003 * k).astype(np.float32)
+    lin["values"] = vals
+    lab, s = orc.sample_tet_labels(lin, TV, T, (0, 0, 0), (1, 1, 1), 0.0, 0.5)
+    c = TV[T].mean(1) / grid["voxel_size"]
+    # lattice cells fully inside active bricks: every sampled voxel is active
+    full = np.zeros(len(T), bool)
+    fi = np.floor(c).astype(np.int64) - grid["origin"]
+    for d in range(8):
+        o = np.array([(d >> 2) & 1, (d >> 1) & 1, d & 1])
+        b = (fi + o) >> 3
+        okb = np.all((b >= 0) & (b < np.array(tab.shape)), 1)
+        act = np.zeros(len(T), bool)
+        act[okb] = tab[tuple(b[okb].T)] >= 0
+        full = act if d == 0 else (full & act)
+    want = 0.001 * c[:, 0] + 0.002 * c[:, 1] + 0.003 * c[:, 2]
+    assert full.sum() > 1000
+    assert np.allclose(s[full], want[full], rtol=0, atol=2e-5)
+    # mesh UDF: sample vs exact centroid distance near the surface
+    lab, s = orc.sample_tet_labels(grid, TV, T, (0, 0, 0), (1, 1, 1), 0.0, 1.0 / 128 - 1e-4)
+    near = s < grid["background"] * 0.6
+    exact0 = synth.udf_labels(TV, T, V, F, 1.0 / 128 - 1e-4)
+    assert near.sum() > 1000
+    # the sampled field interpolates exact voxel distances: labels agree
+    # everywhere except within a voxel of the threshold
+    agree = (lab == exact0).mean()
+    assert agree > 0.97
+    assert set(np.unique(lab)) == {0, 1}
+
+
+def test_label_sampler_oracle_errors():
+    V, F, grid, TV, T = label_case(4)
+    with pytest.raises(RuntimeError, match="degenerate bbox"):
+        orc.sample_tet_labels(grid, TV, T, (0, 0, 0), (1, 0, 1), 0.0, 0.01)
+    bad = T.copy()
+    bad[3, 2] = len(TV)
+    with pytest.raises(RuntimeError, match="tet index out of range"):
+        orc.sample_tet_labels(grid, TV, bad, (0, 0, 0), (1, 1, 1), 0.0, 0.01)

@@ -26,7 +26,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "libwtivo_gpupr.so"
 EXT = PKG / ("wtivo_gpupr" + sysconfig.get_config_var("EXT_SUFFIX"))
 
-CU_SOURCES = ["graph_build.cu", "push_relabel.cu", "batch.cu", "surface.cu", "capi.cu", "server.cu", "hostio.cu", "audit.cu"]
+CU_SOURCES = ["graph_build.cu", "push_relabel.cu", "batch.cu", "surface.cu", "capi.cu", "server.cu", "hostio.cu", "audit.cu", "labels.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

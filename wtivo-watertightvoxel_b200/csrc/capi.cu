@@ -690,6 +690,66 @@ gpupr_status gpupr_edge_audit(const int32_t* faces, uint64_t n_faces, int faces_
     });
 }
 
+gpupr_status gpupr_sample_tet_labels(const gpupr_brick_grid* grid, const double* vertices,
+                                     uint64_t n_vertices, int vertices_on_device,
+                                     const int32_t* tets, uint64_t n_tets, int tets_on_device,
+                                     const double* bbox_min, const double* bbox_max,
+                                     double padding, double threshold, uint8_t* labels_out,
+                                     int labels_on_device, float* udf_out, void* stream)
+{
+    return guarded([&] {
+        if (!grid) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "SparseUDF.sample_tet_labels: grid is empty"};
+        if (!bbox_min || !bbox_max) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "SparseUDF.sample_tet_labels: bbox must have length 3"};
+        if (!(grid->voxel_size > 0.0) || grid->dims[0] < 0 || grid->dims[1] < 0 || grid->dims[2] < 0)
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "invalid brick grid"};
+        const uint64_t cells = (uint64_t)grid->dims[0] * (uint64_t)grid->dims[1] * (uint64_t)grid->dims[2];
+        if (cells && !grid->table) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "invalid brick grid"};
+        if (grid->n_bricks && !grid->values) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "invalid brick grid"};
+        if (n_tets && (!tets || !labels_out || (!vertices && n_vertices)))
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL input"};
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (tets_on_device && n_tets) {
+            if (!aligned(tets, 16)) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets must be 16-byte aligned"};
+            select_device_for(tets, "tets");
+        } else if (grid->on_device && cells) {
+            select_device_for(grid->table, "grid");
+        }
+        DevBuf<int32_t> dtab, dtets;
+        DevBuf<float> dval, dudf;
+        DevBuf<double> dver;
+        DevBuf<uint8_t> dlab;
+        BrickGridDesc g{};
+        g.voxel_size = grid->voxel_size;
+        for (int k = 0; k < 3; ++k) {
+            g.origin[k] = grid->origin[k];
+            g.dims[k] = grid->dims[k];
+        }
+        g.background = grid->background;
+        // the grid is checked before the tets are touched, like the reference
+        g.d_table = on_device(grid->table, cells, grid->on_device, dtab, s);
+        g.d_values = on_device(grid->values, grid->n_bricks * 512u, grid->on_device, dval, s);
+        const double* d_v = on_device(vertices, n_vertices * 3u, vertices_on_device, dver, s);
+        const int32_t* d_t = on_device(tets, n_tets * 4u, tets_on_device, dtets, s);
+        uint8_t* d_l = labels_out;
+        float* d_u = udf_out;
+        if (!labels_on_device && n_tets) {
+            dlab = DevBuf<uint8_t>(n_tets, s);
+            d_l = dlab.p;
+            if (udf_out) {
+                dudf = DevBuf<float>(n_tets, s);
+                d_u = dudf.p;
+            }
+        }
+        sample_tet_labels(g, d_v, n_vertices, d_t, n_tets, bbox_min, bbox_max, padding, threshold, d_l,
+                          d_u, s, nullptr);
+        if (!labels_on_device && n_tets) {
+            device_to_host(labels_out, d_l, n_tets, s);
+            if (udf_out) device_to_host(udf_out, d_u, n_tets * 4u, s);
+        }
+        GPUPR_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 gpupr_status gpupr_release_cached_memory(void)
 {
     return guarded([&] {

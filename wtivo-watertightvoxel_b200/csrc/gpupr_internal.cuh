@@ -249,6 +249,24 @@ void surface_count(const uint8_t* labels, int l_dev, const double* vertices, uin
                    uint64_t* n_used, cudaStream_t s);
 void surface_fetch(int32_t* faces, double* verts, int out_dev, cudaStream_t s);
 
+// Sparse unsigned distance grid of 8^3-voxel bricks in device memory (the
+// layout of gpupr_brick_grid) and the tet-centroid label sampler
+// (labels.cu): labels[i] = 0 where the box-sampled distance at tet i's
+// centroid is <= threshold, else 1; udf (optional) receives the samples.
+struct BrickGridDesc {
+    double voxel_size;
+    int32_t origin[3];
+    int32_t dims[3];
+    float background;
+    const int32_t* d_table;
+    const float* d_values;
+};
+
+void sample_tet_labels(const BrickGridDesc& grid, const double* d_vertices, uint64_t nv,
+                       const int32_t* d_tets, uint64_t nt, const double* bmin, const double* bmax,
+                       double padding, double threshold, uint8_t* d_labels, float* d_udf,
+                       cudaStream_t s, uint64_t* launches);
+
 // Edge-degree watertight audit of F device faces (audit.cu): the number of
 // distinct undirected edges whose face count is not 2, and the bytes of the
 // device edge table used.

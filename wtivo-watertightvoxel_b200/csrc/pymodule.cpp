@@ -254,6 +254,124 @@ py::tuple is_watertight(py::object faces, int threads)
     return py::make_tuple(py::bool_(bad == 0), py::int_(bad), py::float_(sec), py::int_(bytes));
 }
 
+// The UDF side of native/vdb/wtivo_vdb.cpp's SparseUDF, for the label query
+// only: a brick grid (8^3-voxel bricks, a dense brick table, a background)
+// held in device memory as torch tensors, and sample_tet_labels with the
+// reference method's arguments, checks, messages and (labels, seconds)
+// return (wtivo_vdb.cpp:1519-1584).
+class BrickUDF {
+public:
+    BrickUDF(py::object values, py::object table, py::object origin, double voxel_size,
+             float background)
+        : voxel_size_(voxel_size), background_(background)
+    {
+        if (!(voxel_size > 0.0)) throw std::runtime_error("BrickUDF: voxel_size must be > 0");
+        py::module_ np = py::module_::import("numpy");
+        py::module_ torch = py::module_::import("torch");
+        py::array_t<std::int32_t, py::array::c_style | py::array::forcecast> tab =
+            py::array_t<std::int32_t, py::array::c_style | py::array::forcecast>::ensure(table);
+        py::array_t<float, py::array::c_style | py::array::forcecast> val =
+            py::array_t<float, py::array::c_style | py::array::forcecast>::ensure(values);
+        py::array_t<std::int64_t, py::array::c_style | py::array::forcecast> org =
+            py::array_t<std::int64_t, py::array::c_style | py::array::forcecast>::ensure(origin);
+        if (!tab || tab.ndim() != 3) throw std::runtime_error("BrickUDF: table must be int32 [bx, by, bz]");
+        if (!val || val.size() % 512 != 0) throw std::runtime_error("BrickUDF: values must be float32 [bricks, 8, 8, 8]");
+        if (!org || org.size() != 3) throw std::runtime_error("BrickUDF: origin must have length 3");
+        for (int k = 0; k < 3; ++k) {
+            dims_[k] = (int32_t)tab.shape(k);
+            origin_[k] = (int32_t)org.data()[k];
+        }
+        n_bricks_ = (std::uint64_t)(val.size() / 512);
+        const std::int32_t* tp = tab.data();
+        for (py::ssize_t i = 0; i < tab.size(); ++i)
+            if (tp[i] < -1 || (tp[i] >= 0 && (std::uint64_t)tp[i] >= n_bricks_))
+                throw std::runtime_error("BrickUDF: table entry out of range");
+        table_ = torch.attr("from_numpy")(tab.attr("reshape")(-1)).attr("cuda")();
+        values_ = torch.attr("from_numpy")(val.attr("reshape")(-1)).attr("cuda")();
+    }
+
+    py::tuple sample_tet_labels(py::object tet_vertices, py::object tets, py::object bbox_min,
+                                py::object bbox_max, double padding, double threshold, int threads)
+    {
+        (void)threads;
+        const std::string pre = "SparseUDF.sample_tet_labels: ";
+        py::module_ torch = py::module_::import("torch");
+        F64 V = F64::ensure(tet_vertices);
+        if (!V || V.ndim() != 2 || V.shape(1) != 3)
+            throw std::runtime_error(pre + "tet_vertices must be float64 Nx3");
+        const int32_t* tp = nullptr;
+        std::uint64_t nt = 0;
+        int t_dev = 0;
+        py::object keep;
+        if (py::isinstance(tets, torch.attr("Tensor")) && tets.attr("is_cuda").cast<bool>()) {
+            if (!py::object(tets.attr("dtype")).equal(torch.attr("int32")) || tets.attr("dim")().cast<int64_t>() != 2 ||
+                tets.attr("size")(1).cast<int64_t>() != 4 || !tets.attr("is_contiguous")().cast<bool>())
+                throw std::runtime_error(pre + "tets must be int32 Mx4");
+            nt = tets.attr("size")(0).cast<std::uint64_t>();
+            tp = reinterpret_cast<const int32_t*>(tets.attr("data_ptr")().cast<uintptr_t>());
+            t_dev = 1;
+            keep = tets;
+        } else {
+            py::array_t<std::int32_t, py::array::c_style | py::array::forcecast> T =
+                py::array_t<std::int32_t, py::array::c_style | py::array::forcecast>::ensure(tets);
+            if (!T || T.ndim() != 2 || T.shape(1) != 4) throw std::runtime_error(pre + "tets must be int32 Mx4");
+            nt = (std::uint64_t)T.shape(0);
+            tp = T.data();
+            keep = T;
+        }
+        F64 bmin = F64::ensure(bbox_min), bmax = F64::ensure(bbox_max);
+        if (!bmin || !bmax || bmin.ndim() != 1 || bmin.shape(0) != 3 || bmax.ndim() != 1 || bmax.shape(0) != 3)
+            throw std::runtime_error(pre + "bbox must have length 3");
+        py::array_t<std::uint8_t> labels(static_cast<py::ssize_t>(nt));
+        gpupr_brick_grid g{};
+        g.voxel_size = voxel_size_;
+        for (int k = 0; k < 3; ++k) {
+            g.origin[k] = origin_[k];
+            g.dims[k] = dims_[k];
+        }
+        g.background = background_;
+        g.on_device = 1;
+        g.table = reinterpret_cast<const int32_t*>(table_.attr("data_ptr")().cast<uintptr_t>());
+        g.values = reinterpret_cast<const float*>(values_.attr("data_ptr")().cast<uintptr_t>());
+        g.n_bricks = n_bricks_;
+        void* stream = current_stream(table_.attr("device").attr("index").cast<int>());
+        const double* vp = V.data();
+        const std::uint64_t nv = (std::uint64_t)V.shape(0);
+        const double* b0 = bmin.data();
+        const double* b1 = bmax.data();
+        std::uint8_t* lp = labels.mutable_data();
+        const auto t0 = std::chrono::steady_clock::now();
+        gpupr_status rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = gpupr_sample_tet_labels(&g, vp, nv, 0, tp, nt, t_dev, b0, b1, padding, threshold, lp, 0,
+                                         nullptr, stream);
+        }
+        if (rc != GPUPR_OK) raise_status(rc);
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return py::make_tuple(labels, sec);
+    }
+
+    py::dict stats() const
+    {
+        py::dict d;
+        d["voxel_size"] = voxel_size_;
+        d["background"] = background_;
+        d["bricks"] = n_bricks_;
+        d["dims"] = py::make_tuple(dims_[0], dims_[1], dims_[2]);
+        d["origin"] = py::make_tuple(origin_[0], origin_[1], origin_[2]);
+        d["device_bytes"] = (std::uint64_t)(n_bricks_ * 2048u + (std::uint64_t)dims_[0] * dims_[1] * dims_[2] * 4u);
+        return d;
+    }
+
+private:
+    double voxel_size_;
+    float background_;
+    int32_t origin_[3] = {0, 0, 0}, dims_[3] = {0, 0, 0};
+    std::uint64_t n_bricks_ = 0;
+    py::object table_, values_;
+};
+
 py::dict last_stats()
 {
     const gpupr_cut_stats& s = t_last;
@@ -298,6 +416,15 @@ PYBIND11_MODULE(wtivo_gpupr, m)
     m.def("surface_extraction_topology_cuda", &surface_extraction_topology_cuda, py::arg("labels"),
           py::arg("vertices"), py::arg("tets_cuda"), py::arg("neighbors_cuda"),
           py::arg("threads") = 16);
+    py::class_<BrickUDF>(m, "BrickUDF",
+                         "Sparse unsigned distance grid (8^3-voxel bricks) on the GPU for the "
+                         "tet-centroid label query (replaces SparseUDF.sample_tet_labels).")
+        .def(py::init<py::object, py::object, py::object, double, float>(), py::arg("values"),
+             py::arg("table"), py::arg("origin"), py::arg("voxel_size"), py::arg("background"))
+        .def("sample_tet_labels", &BrickUDF::sample_tet_labels, py::arg("tet_vertices"), py::arg("tets"),
+             py::arg("bbox_min"), py::arg("bbox_max"), py::arg("padding"), py::arg("threshold"),
+             py::arg("threads") = 16)
+        .def("stats", &BrickUDF::stats);
     m.def("is_watertight", &is_watertight, py::arg("faces"), py::arg("threads") = 0,
           "Edge-degree watertight audit on the GPU (replaces wtivo_core.is_watertight).");
     m.def("topology_to_cuda_chunked", &topology_to_cuda_chunked, py::arg("host_array"),

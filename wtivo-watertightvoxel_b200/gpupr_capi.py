@@ -126,6 +126,8 @@ def lib():
                                             ctypes.c_int32, p, p]
         L.gpupr_edge_audit.argtypes = [p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                        ctypes.POINTER(ctypes.c_uint64), p]
+        L.gpupr_sample_tet_labels.argtypes = [p, p, ctypes.c_uint64, ctypes.c_int, p, ctypes.c_uint64,
+                                              ctypes.c_int, p, p, f64, f64, p, ctypes.c_int, p, p]
         L.gpupr_release_cached_memory.argtypes = []
         L.gpupr_selftest_bounded_wait.argtypes = [ctypes.c_uint32, p]
         for name in header_functions():
@@ -404,6 +406,52 @@ def edge_audit(faces):
         check(lib().gpupr_edge_audit(_hp(f), f.shape[0], 0, ctypes.byref(bad), ctypes.byref(nbytes),
                                      _stream(torch)))
     return int(bad.value), int(nbytes.value)
+
+
+class BrickGrid(ctypes.Structure):
+    _fields_ = [("voxel_size", ctypes.c_double), ("origin", ctypes.c_int32 * 3),
+                ("dims", ctypes.c_int32 * 3), ("background", ctypes.c_float),
+                ("on_device", ctypes.c_int32), ("table", ctypes.c_void_p), ("values", ctypes.c_void_p),
+                ("n_bricks", ctypes.c_uint64)]
+
+
+def sample_tet_labels(grid, vertices, tets, bbox_min, bbox_max, padding, threshold, device_out=False):
+    """gpupr_sample_tet_labels.  grid: dict as made by synth.brick_udf (host
+    arrays, or CUDA tensors for table/values).  vertices/tets: numpy or CUDA.
+    Returns (labels, samples) (numpy, or CUDA tensors with device_out)."""
+    import torch
+
+    tab, val = grid["table"], grid["values"]
+    g_dev = isinstance(tab, torch.Tensor)
+    if not g_dev:
+        tab = np.ascontiguousarray(tab, np.int32)
+        val = np.ascontiguousarray(val, np.float32)
+    g = BrickGrid(float(grid["voxel_size"]), (ctypes.c_int32 * 3)(*[int(x) for x in grid["origin"]]),
+                  (ctypes.c_int32 * 3)(*[int(x) for x in grid["dims"]]), float(grid["background"]), int(g_dev),
+                  _dp(tab) if g_dev else _hp(tab), _dp(val) if g_dev else _hp(val),
+                  int((val.numel() if g_dev else val.size) // 512))
+    v_dev = isinstance(vertices, torch.Tensor)
+    t_dev = isinstance(tets, torch.Tensor)
+    if not v_dev:
+        vertices = np.ascontiguousarray(vertices, np.float64)
+    if not t_dev:
+        tets = np.ascontiguousarray(tets, np.int32)
+    n = int(tets.shape[0])
+    if device_out:
+        dev = tets.device if t_dev else torch.device("cuda")
+        lab = torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
+        udf = torch.empty(max(n, 1), dtype=torch.float32, device=dev)
+    else:
+        lab = np.empty(max(n, 1), np.uint8)
+        udf = np.empty(max(n, 1), np.float32)
+    bmin = np.ascontiguousarray(bbox_min, np.float64)
+    bmax = np.ascontiguousarray(bbox_max, np.float64)
+    check(lib().gpupr_sample_tet_labels(
+        ctypes.byref(g), _dp(vertices) if v_dev else _hp(vertices), int(vertices.shape[0]), int(v_dev),
+        _dp(tets) if t_dev else _hp(tets), n, int(t_dev), _hp(bmin), _hp(bmax), float(padding),
+        float(threshold), _dp(lab) if device_out else _hp(lab), int(device_out),
+        _dp(udf) if device_out else _hp(udf), _stream(torch, tets.device if t_dev else None)))
+    return lab[:n], udf[:n]
 
 
 def release_cached_memory():

@@ -333,3 +333,78 @@ int synth_udf_labels(const double* V, int64_t nv, const int32_t* tets, int64_t N
     free(MV);
     return 0;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Narrow-band unsigned distance on a brick grid: the input of the tet-    */
+/* centroid label sampler, standing in for OpenVDB's                       */
+/* meshToUnsignedDistanceField (the reference's SparseUDF,                 */
+/* native/vdb/wtivo_vdb.cpp:1007-1070, linear transform of voxel size h).  */
+/* Voxel (i,j,k) sits at world (i,j,k)*h; a voxel closer than band to a    */
+/* triangle holds its exact distance to the mesh (float), every other      */
+/* voxel the background band.  Bricks are 8^3 voxels; the brick box is     */
+/* [bmin3, bmin3 + dims) in brick units (voxel index >> 3).                */
+/*   mode 0: mask[dims] = 1 for every brick a triangle's band box touches; */
+/*   mode 1: values[brick][8][8][8] (z fastest, preset to the background   */
+/*           by the caller) get the distances, through table[dims]         */
+/*           (brick number, -1 = inactive).                                */
+/* Returns 0, or -1 on a voxel outside the brick box.                      */
+/* ---------------------------------------------------------------------- */
+static void atomic_min_nonneg_float(float* p, float v)
+{
+    uint32_t nv_bits, old;
+    memcpy(&nv_bits, &v, 4);
+    uint32_t* q = (uint32_t*)p;
+    old = __atomic_load_n(q, __ATOMIC_RELAXED);
+    /* non-negative floats order like their bit patterns */
+    while (nv_bits < old &&
+           !__atomic_compare_exchange_n(q, &old, nv_bits, 1, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+    }
+}
+
+int synth_brick_udf(const double* MV, int64_t nv, const int32_t* MF, int64_t nf, double h,
+                    double band, const int32_t* bmin3, const int32_t* dims, int mode,
+                    uint8_t* mask, const int32_t* table, float* values)
+{
+    (void)nv;
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(| : bad)
+    for (int64_t f = 0; f < nf; ++f) {
+        const double* a = MV + (size_t)MF[f * 3] * 3;
+        const double* b = MV + (size_t)MF[f * 3 + 1] * 3;
+        const double* c = MV + (size_t)MF[f * 3 + 2] * 3;
+        int64_t lo[3], hi[3];
+        for (int k = 0; k < 3; ++k) {
+            double mn = a[k], mx = a[k];
+            if (b[k] < mn) mn = b[k];
+            if (c[k] < mn) mn = c[k];
+            if (b[k] > mx) mx = b[k];
+            if (c[k] > mx) mx = c[k];
+            lo[k] = (int64_t)ceil((mn - band) / h);
+            hi[k] = (int64_t)floor((mx + band) / h);
+        }
+        for (int k = 0; k < 3; ++k)
+            if ((lo[k] >> 3) < bmin3[k] || (hi[k] >> 3) >= (int64_t)bmin3[k] + dims[k]) bad = 1;
+        if (bad) continue;
+        if (mode == 0) {
+            for (int64_t x = lo[0] >> 3; x <= hi[0] >> 3; ++x)
+                for (int64_t y = lo[1] >> 3; y <= hi[1] >> 3; ++y)
+                    for (int64_t z = lo[2] >> 3; z <= hi[2] >> 3; ++z)
+                        mask[((x - bmin3[0]) * dims[1] + (y - bmin3[1])) * dims[2] + (z - bmin3[2])] = 1;
+            continue;
+        }
+        for (int64_t x = lo[0]; x <= hi[0]; ++x)
+            for (int64_t y = lo[1]; y <= hi[1]; ++y)
+                for (int64_t z = lo[2]; z <= hi[2]; ++z) {
+                    const double p[3] = {(double)x * h, (double)y * h, (double)z * h};
+                    const double d = sqrt(pt_tri_d2(p, a, b, c));
+                    if (!(d < band)) continue;
+                    const int64_t bi = ((((x >> 3) - bmin3[0]) * dims[1] + ((y >> 3) - bmin3[1])) * dims[2] +
+                                        ((z >> 3) - bmin3[2]));
+                    const int32_t brick = table[bi];
+                    if (brick < 0) continue;
+                    atomic_min_nonneg_float(values + (size_t)brick * 512 + ((x & 7) * 8 + (y & 7)) * 8 + (z & 7),
+                                            (float)d);
+                }
+    }
+    return bad ? -1 : 0;
+}
