@@ -460,6 +460,7 @@ def config2(seed: int = 0, n_tets: int = 80_000_000, n_faces: int = 2_000_000):
     g = lattice_graph(mv, mf, n_tets, seed + 1)
     g["fill_T"] = 10.0
     g["name"] = f"torusknot-lattice-{g.n_tets}"
+    g["mesh_V"], g["mesh_F"] = mv, mf
     return g
 
 
