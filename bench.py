@@ -167,9 +167,17 @@ def max_over_ranks(x, world):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job(units_per_rank, ms_local, world):
+    """Weak-scaling aggregate: every rank processed units_per_rank in
+    ms_local; the job took the slowest rank's time.  Returns (ms, units/s)."""
+    ms = max_over_ranks(ms_local, world)
+    return ms, world * units_per_rank / (ms * 1e-3)
 
 
 def make_graph(n_tets, seed):
@@ -239,7 +247,7 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         barrier(world)
     ms = e0.elapsed_time(e1) / args.steps
-    ms_max = max_over_ranks(ms, world)
+    ms_max, value = whole_job(N, ms, world)
     clocks = clk.summary()
 
     # roofline of the dominant kernel, from the same timed steps
@@ -288,30 +296,76 @@ def run_ours(args, world, rank, local):
         pn = torch.from_numpy(g["neighbors"]).pin_memory()
         hV = np.ascontiguousarray(g["vertices"])
         hL = np.ascontiguousarray(g["labels"])
-        dt_ = torch.empty_like(tets)
-        dn_ = torch.empty_like(nbrs)
+        # double-buffered topology: step k+1's upload runs on a copy stream
+        # while step k cuts (every step still copies its own inputs in).
+        # Both are non-default streams: work on the legacy default stream
+        # would wait for every other stream and serialise the two.
+        bufs = [(torch.empty_like(tets), torch.empty_like(nbrs)) for _ in range(2)]
+        copy_stream = torch.cuda.Stream(dev)
+        cut_stream = torch.cuda.Stream(dev)
+        ready = [torch.cuda.Event(), torch.cuda.Event()]
 
-        def e2e_step():
-            dt_.copy_(pt, non_blocking=True)
-            dn_.copy_(pn, non_blocking=True)
-            r = wtivo_gpupr.graph_cut_fast(hV, dt_, dn_, hL, 10.0)
-            return r
+        def upload(k):
+            """Step k's topology, in 64 MiB pieces with at most one piece in
+            the copy queue, so the cut's own host copies are never queued
+            behind gigabytes of it (runs on a host thread during the cut)."""
+            dt_, dn_ = bufs[k % 2]
+            copy_stream.wait_stream(cut_stream)
+            piece = torch.cuda.Event()
+            rows = 1 << 22
+            with torch.cuda.stream(copy_stream):
+                for i in range(0, pt.shape[0], rows):
+                    dt_[i:i + rows].copy_(pt[i:i + rows], non_blocking=True)
+                    dn_[i:i + rows].copy_(pn[i:i + rows], non_blocking=True)
+                    piece.record(copy_stream)
+                    piece.synchronize()
+                ready[k % 2].record(copy_stream)
 
-        e2e_step()
+        def cut(k):
+            cut_stream.wait_event(ready[k % 2])
+            dt_, dn_ = bufs[k % 2]
+            with torch.cuda.stream(cut_stream):   # the module runs on the current stream
+                return wtivo_gpupr.graph_cut_fast(hV, dt_, dn_, hL, 10.0)
+
+        def serial_step():
+            upload(0)
+            return cut(0)
+
+        import threading
+
+        serial_step()
         torch.cuda.synchronize()
-        barrier(world)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
+        barrier(world)
+        a.record(cut_stream)
         for _ in range(args.steps):
-            r = e2e_step()
-        b.record(stream)
+            r = serial_step()
+        b.record(cut_stream)
         torch.cuda.synchronize()
-        ems = max_over_ranks(a.elapsed_time(b) / args.steps, world)
+        serial_ms = a.elapsed_time(b) / args.steps
+        barrier(world)
+        a.record(cut_stream)
+        upload(0)
+        for k in range(args.steps):
+            th = None
+            if k + 1 < args.steps:
+                th = threading.Thread(target=upload, args=(k + 1,))
+                th.start()
+            r = cut(k)
+            if th is not None:
+                th.join()
+        b.record(cut_stream)
+        torch.cuda.synchronize()
+        ems, evalue = whole_job(N, a.elapsed_time(b) / args.steps, world)
+        serial_ms = max_over_ranks(serial_ms, world)
         h2d = pt.numel() * 4 + pn.numel() * 4 + hV.nbytes + hL.nbytes
-        e2e = {"value": round(world * N / (ems * 1e-3), 1), "unit": "tets/s",
+        e2e = {"value": round(evalue, 1), "unit": "tets/s",
                "ms_per_step": round(ems, 3), "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(N),
-               "api": "wtivo_gpupr.graph_cut_fast (host vertices/labels, pinned topology copies)"}
+               "serial_ms_per_step": round(serial_ms, 3),
+               "api": "wtivo_gpupr.graph_cut_fast with host vertices/labels and labels returned to "
+                      "numpy; each step's tets/neighbors copied from pinned memory, step k+1's copy "
+                      "on a second stream while step k cuts (serial_ms_per_step: no overlap)"}
         assert np.array_equal(np.asarray(r[0]), out.cpu().numpy()), "e2e labels differ"
 
     cpu = None
@@ -324,7 +378,7 @@ def run_ours(args, world, rank, local):
 
     s0 = stats[-1]
     line = {
-        "metric": METRIC, "value": round(world * N / (ms_max * 1e-3), 1), "unit": "tets/s",
+        "metric": METRIC, "value": round(value, 1), "unit": "tets/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_max, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64 (exact integer flow; FP64 capacities)",
