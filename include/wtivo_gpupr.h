@@ -76,6 +76,8 @@ typedef struct {
     uint64_t discharge_launches;
     uint64_t bfs_launches;
     int64_t engine;             /* 1 one launch per step, 2 persistent */
+    int64_t solve_blocks_per_sm;/* persistent engine: resident blocks per SM used */
+    double relabel_work_factor; /* persistent engine: relabel work factor used */
 } gpupr_cut_stats;
 
 /* Solver tuning knobs; zero fields take the defaults shown. */
@@ -378,6 +380,35 @@ gpupr_status gpupr_sample_tet_labels(const gpupr_brick_grid* grid, const double*
                                      const double* bbox_min, const double* bbox_max,
                                      double padding, double threshold, uint8_t* labels_out,
                                      int labels_on_device, float* udf_out, void* stream);
+
+/*
+ * Autotuner (no counterpart in the reference).  The persistent engine's two
+ * free choices -- resident blocks per SM and the relabel work factor -- change
+ * the time of a solve, never its result.  gpupr_autotune builds the reduced
+ * graph of the given cut once, then times the solve (restoring the graph each
+ * time) under every pair of blocks per SM {1,2,3,4} and work factor
+ * {0.5,1,2}, `reps` times each (default 3), interleaved, and keeps the pair
+ * with the lowest median for the graph's size class (free nodes in
+ * [2^k, 2^(k+1))).  Later solves whose options leave those fields at 0 use
+ * the table; classes without an entry keep the built-in size rule.  The
+ * table is per process; gpupr_tune_table / gpupr_tune_table_set read and
+ * replace it (to keep it across runs).  Arguments as gpupr_graph_cut.
+ */
+typedef struct {
+    int32_t size_class;           /* k: free nodes in [2^k, 2^(k+1)) */
+    int32_t blocks_per_sm;
+    double work_relabel_factor;
+    double solve_ms;              /* median solve time of the chosen pair */
+    double default_ms;            /* median solve time under the built-in rule */
+} gpupr_tune_entry;
+
+gpupr_status gpupr_autotune(const double* vertices, uint64_t n_vertices, int vertices_on_device,
+                            const int32_t* d_tets, const int32_t* d_neighbors, uint64_t n_tets,
+                            const uint8_t* labels, int labels_on_device, double fill_T,
+                            int32_t local_steps, int32_t reps, gpupr_tune_entry* chosen,
+                            void* stream);
+gpupr_status gpupr_tune_table(gpupr_tune_entry* entries, uint32_t capacity, uint32_t* count);
+gpupr_status gpupr_tune_table_set(const gpupr_tune_entry* entries, uint32_t count);
 
 /* Release device memory cached between calls (pool + scratch). */
 gpupr_status gpupr_release_cached_memory(void);

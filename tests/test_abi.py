@@ -114,3 +114,26 @@ def test_is_watertight_checks_before_the_gpu(built):
     with pytest.raises(RuntimeError, match="is_watertight expects Fx3 int32 faces"):
         wtivo_gpupr.is_watertight(np.zeros(9, np.int32))
     assert wtivo_gpupr.is_watertight(np.zeros((0, 3), np.int32), 16) == (False, 0, 0.0, 0)
+
+
+def test_tune_table_round_trip(built, tmp_path):
+    """The autotuner's table is host state: set, read back, save/load,
+    reject invalid entries, clear."""
+    import gpupr_capi
+
+    entries = [dict(size_class=18, blocks_per_sm=1, work_relabel_factor=2.0, solve_ms=10.0, default_ms=11.0),
+               dict(size_class=26, blocks_per_sm=4, work_relabel_factor=0.5, solve_ms=120.0, default_ms=130.0)]
+    gpupr_capi.set_tune_table(entries)
+    assert gpupr_capi.tune_table() == entries
+    p = tmp_path / "tune.json"
+    gpupr_capi.save_tune_table(p)
+    gpupr_capi.set_tune_table([])
+    assert gpupr_capi.tune_table() == []
+    gpupr_capi.load_tune_table(p)
+    assert gpupr_capi.tune_table() == entries
+    for bad in (dict(entries[0], blocks_per_sm=0), dict(entries[0], size_class=40),
+                dict(entries[0], work_relabel_factor=0.0)):
+        with pytest.raises(gpupr_capi.GpuprError):
+            gpupr_capi.set_tune_table([bad])
+    assert gpupr_capi.tune_table() == entries        # a rejected set changes nothing
+    gpupr_capi.set_tune_table([])

@@ -211,8 +211,85 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
     st->discharge_launches = sr.discharge_launches;
     st->bfs_launches = sr.bfs_launches;
     st->engine = sr.engine;
+    st->solve_blocks_per_sm = sr.blocks_per_sm;
+    st->relabel_work_factor = sr.work_factor;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
+}
+
+// gpupr_autotune: one build, then timed solves of the same reduced graph
+// (residuals and terminals restored before each) under every candidate pair,
+// interleaved so slow drifts of the clock hit every pair alike.
+TuneEntry run_autotune(const double* vertices, uint64_t nv, int v_dev, const int32_t* d_tets,
+                       const int32_t* d_nbrs, uint64_t N, const uint8_t* labels, int l_dev,
+                       double fill_T, int32_t local_steps, int32_t reps, cudaStream_t s)
+{
+    if (N == 0 || N > 0xFFFFFFFFull) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "autotune needs 1..2^32-1 tets"};
+    if (!d_tets || !d_nbrs || !labels || (!vertices && nv))
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL input"};
+    if (!aligned(d_tets, 16) || !aligned(d_nbrs, 16))
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets/neighbors must be 16-byte aligned"};
+    select_device_for(d_tets, "tets/neighbors");
+    if (reps <= 0) reps = 3;
+    if (reps > 50) reps = 50;
+    DevBuf<uint8_t> dlab;
+    DevBuf<double> dver;
+    const uint8_t* d_labels = on_device(labels, N, l_dev, dlab, s);
+    const double* d_vertices = on_device(vertices, nv * 3u, v_dev, dver, s);
+    BuildInputs in{d_vertices, nv, d_tets, d_nbrs, d_labels, N, fill_T};
+    ReducedGraph g;
+    BuildInfo info;
+    uint64_t launches = 0;
+    build_reduced_graph(in, g, info, s, &launches);
+    if (info.free_n == 0) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "autotune: the cut has no free tet"};
+    DevBuf<uint32_t> res0(4u * (size_t)g.n, s);
+    DevBuf<int32_t> term0(g.n, s);
+    GPUPR_CUDA(cudaMemcpyAsync(res0.p, g.res.p, 16u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+    GPUPR_CUDA(cudaMemcpyAsync(term0.p, g.term.p, 4u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+    struct Cand {
+        int bps;
+        double wf;
+        std::vector<double> ms;
+    };
+    std::vector<Cand> cands;
+    cands.push_back({0, 0.0, {}});   // the built-in rule
+    for (int b : {1, 2, 3, 4})
+        for (double f : {0.5, 1.0, 2.0}) cands.push_back({b, f, {}});
+    SolveWorkspace w;
+    for (int r = 0; r < reps; ++r)
+        for (Cand& c : cands) {
+            GPUPR_CUDA(cudaMemcpyAsync(g.res.p, res0.p, 16u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+            GPUPR_CUDA(cudaMemcpyAsync(g.term.p, term0.p, 4u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+            gpupr_solve_options o{};
+            o.local_steps = local_steps;
+            o.engine = 2;
+            o.blocks_per_sm = c.bps;
+            o.work_relabel_factor = c.wf;
+            SolveOptions opt = resolve_options(&o, local_steps, 1024, 2000000ull);
+            SolveResult sr;
+            solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.term.p, w, opt, s, sr);
+            c.ms.push_back(sr.solve_device_ms);
+        }
+    auto median = [](std::vector<double> v) {
+        std::sort(v.begin(), v.end());
+        return v.size() % 2 ? v[v.size() / 2] : 0.5 * (v[v.size() / 2 - 1] + v[v.size() / 2]);
+    };
+    TuneEntry best;
+    best.size_class = size_class(g.n);
+    double best_ms = 1e300;
+    for (const Cand& c : cands) {
+        if (c.bps == 0) continue;
+        const double m = median(c.ms);
+        if (m < best_ms) {
+            best_ms = m;
+            best.blocks_per_sm = c.bps;
+            best.work_factor = c.wf;
+        }
+    }
+    best.solve_ms = best_ms;
+    best.default_ms = median(cands[0].ms);
+    tune_store(best);
+    return best;
 }
 
 }  // namespace
@@ -332,6 +409,8 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     st->discharge_ms = sr.discharge_ms;
     st->bfs_ms = sr.bfs_ms;
     st->engine = sr.engine;
+    st->solve_blocks_per_sm = sr.blocks_per_sm;
+    st->relabel_work_factor = sr.work_factor;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -536,6 +615,8 @@ gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_r
             stats->discharge_launches = sr.discharge_launches;
             stats->bfs_launches = sr.bfs_launches;
             stats->engine = sr.engine;
+            stats->solve_blocks_per_sm = sr.blocks_per_sm;
+            stats->relabel_work_factor = sr.work_factor;
             stats->kernel_launches = launches;
         }
     });
@@ -592,6 +673,8 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
             stats->discharge_launches = sr.discharge_launches;
             stats->bfs_launches = sr.bfs_launches;
             stats->engine = sr.engine;
+            stats->solve_blocks_per_sm = sr.blocks_per_sm;
+            stats->relabel_work_factor = sr.work_factor;
             stats->kernel_launches = launches;
         }
     });
@@ -747,6 +830,59 @@ gpupr_status gpupr_sample_tet_labels(const gpupr_brick_grid* grid, const double*
             if (udf_out) device_to_host(udf_out, d_u, n_tets * 4u, s);
         }
         GPUPR_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+gpupr_status gpupr_autotune(const double* vertices, uint64_t n_vertices, int vertices_on_device,
+                            const int32_t* d_tets, const int32_t* d_neighbors, uint64_t n_tets,
+                            const uint8_t* labels, int labels_on_device, double fill_T,
+                            int32_t local_steps, int32_t reps, gpupr_tune_entry* chosen,
+                            void* stream)
+{
+    return guarded([&] {
+        const TuneEntry e = run_autotune(vertices, n_vertices, vertices_on_device, d_tets, d_neighbors,
+                                         n_tets, labels, labels_on_device, fill_T,
+                                         local_steps > 0 ? local_steps : 8, reps,
+                                         static_cast<cudaStream_t>(stream));
+        if (chosen) {
+            chosen->size_class = e.size_class;
+            chosen->blocks_per_sm = e.blocks_per_sm;
+            chosen->work_relabel_factor = e.work_factor;
+            chosen->solve_ms = e.solve_ms;
+            chosen->default_ms = e.default_ms;
+        }
+    });
+}
+
+gpupr_status gpupr_tune_table(gpupr_tune_entry* entries, uint32_t capacity, uint32_t* count)
+{
+    return guarded([&] {
+        if (!count) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "count pointer is NULL"};
+        const std::vector<TuneEntry> all = tune_all();
+        *count = (uint32_t)all.size();
+        for (uint32_t i = 0; i < all.size() && i < capacity && entries; ++i) {
+            entries[i].size_class = all[i].size_class;
+            entries[i].blocks_per_sm = all[i].blocks_per_sm;
+            entries[i].work_relabel_factor = all[i].work_factor;
+            entries[i].solve_ms = all[i].solve_ms;
+            entries[i].default_ms = all[i].default_ms;
+        }
+    });
+}
+
+gpupr_status gpupr_tune_table_set(const gpupr_tune_entry* entries, uint32_t count)
+{
+    return guarded([&] {
+        if (count && !entries) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "entries pointer is NULL"};
+        std::vector<TuneEntry> v(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            v[i].size_class = entries[i].size_class;
+            v[i].blocks_per_sm = entries[i].blocks_per_sm;
+            v[i].work_factor = entries[i].work_relabel_factor;
+            v[i].solve_ms = entries[i].solve_ms;
+            v[i].default_ms = entries[i].default_ms;
+        }
+        tune_replace(v);
     });
 }
 

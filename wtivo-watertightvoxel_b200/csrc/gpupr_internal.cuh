@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "wtivo_gpupr.h"
 
@@ -233,7 +234,21 @@ struct SolveResult {
     uint64_t discharge_launches = 0, bfs_launches = 0;
     uint64_t workspace_bytes = 0;
     int engine = 1;                // 1 one launch per step, 2 persistent
+    int blocks_per_sm = 0;         // persistent engine: grid used
+    double work_factor = 0.0;      // persistent engine: relabel work factor used
 };
+
+// Autotuner table (push_relabel.cu): per size class (floor(log2 n)), the
+// persistent engine's blocks per SM and relabel work factor.
+struct TuneEntry {
+    int32_t size_class = 0, blocks_per_sm = 0;
+    double work_factor = 0.0, solve_ms = 0.0, default_ms = 0.0;
+};
+bool tune_lookup(uint32_t n, TuneEntry* out);
+void tune_store(const TuneEntry& e);
+std::vector<TuneEntry> tune_all();
+void tune_replace(const std::vector<TuneEntry>& entries);
+int size_class(uint32_t n);
 
 // Phase-I push-relabel on a reduced graph (res/term updated in place).
 // On return the workspace heights mark the sink-reachable set

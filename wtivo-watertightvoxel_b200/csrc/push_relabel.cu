@@ -656,12 +656,17 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     // number of blocks, while a large graph needs the threads to cover its
     // frontiers (measured on B200: 1 is best below ~1.5M free nodes, 4 at
     // ~77M)
+    // An autotuned entry for this size class replaces the rule.
+    TuneEntry te;
+    const bool tuned = tune_lookup(g.n, &te);
     const int want = opt.blocks_per_sm > 0 ? opt.blocks_per_sm
-                     : g.n < 1500000u     ? 1
-                     : g.n < 6000000u     ? 2
-                     : g.n < 40000000u    ? 3
-                                          : 4;
-    const unsigned grid = (unsigned)(sm_count() * (want < bps ? want : bps));
+                     : tuned                ? te.blocks_per_sm
+                     : g.n < 1500000u       ? 1
+                     : g.n < 6000000u       ? 2
+                     : g.n < 40000000u      ? 3
+                                            : 4;
+    const int used = want < bps ? want : bps;
+    const unsigned grid = (unsigned)(sm_count() * used);
     PersistParams p{};
     p.max_rounds = opt.max_rounds;
     // Global relabels: a discharge phase ends once its node visits exceed
@@ -670,7 +675,10 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     // work rule normally reaches first.  The result does not depend on this
     // schedule: the solve always ends with an exact relabel.
     p.relabel_rounds = (uint32_t)(opt.period > 0 ? opt.period : 0);
-    const double wf = opt.work_factor > 0 ? opt.work_factor : (g.n < 500000u ? 2.0 : 1.0);
+    const double wf = opt.work_factor > 0 ? opt.work_factor
+                      : tuned                ? te.work_factor
+                      : g.n < 500000u        ? 2.0
+                                             : 1.0;
     const double budget = wf * (double)g.n;
     p.budget = budget > 1.8e19 ? 0ull : (unsigned long long)budget;
     p.limit_ns = (unsigned long long)(opt.time_limit_s * 1e9);
@@ -699,6 +707,8 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     float ms = 0.f;
     GPUPR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     out.engine = 2;
+    out.blocks_per_sm = used;
+    out.work_factor = wf;
     out.launches = 1;
     out.raw_flow = (int64_t)hc.sink_flow;
     out.rounds = hc.rounds_done;
@@ -1049,6 +1059,66 @@ void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t*
     out.pushes = hc.pushes;
     out.bfs_visits = hc.bfs_visits;
     out.solve_s = std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner table: one entry per size class, shared by the process.
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_tune_mu;
+TuneEntry g_tune[33];
+bool g_tune_valid[33] = {};
+
+bool valid_entry(const TuneEntry& e)
+{
+    return e.size_class >= 0 && e.size_class <= 32 && e.blocks_per_sm >= 1 && e.blocks_per_sm <= 32 &&
+           e.work_factor > 0.0 && e.work_factor < 1e6;
+}
+}  // namespace
+
+int size_class(uint32_t n)
+{
+    int k = 0;
+    while (k < 31 && (n >> (k + 1)) != 0u) ++k;
+    return k;
+}
+
+bool tune_lookup(uint32_t n, TuneEntry* out)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    const int k = size_class(n);
+    if (!g_tune_valid[k]) return false;
+    *out = g_tune[k];
+    return true;
+}
+
+void tune_store(const TuneEntry& e)
+{
+    if (!valid_entry(e)) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "invalid tuning entry"};
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[e.size_class] = e;
+    g_tune_valid[e.size_class] = true;
+}
+
+std::vector<TuneEntry> tune_all()
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::vector<TuneEntry> v;
+    for (int k = 0; k <= 32; ++k)
+        if (g_tune_valid[k]) v.push_back(g_tune[k]);
+    return v;
+}
+
+void tune_replace(const std::vector<TuneEntry>& entries)
+{
+    for (const TuneEntry& e : entries)
+        if (!valid_entry(e)) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "invalid tuning entry"};
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (int k = 0; k <= 32; ++k) g_tune_valid[k] = false;
+    for (const TuneEntry& e : entries) {
+        g_tune[e.size_class] = e;
+        g_tune_valid[e.size_class] = true;
+    }
 }
 
 }  // namespace gpupr

@@ -35,6 +35,7 @@ STATS_FIELDS = [
     ("build_device_ms", ctypes.c_double), ("discharge_ms", ctypes.c_double),
     ("bfs_ms", ctypes.c_double), ("discharge_launches", ctypes.c_uint64),
     ("bfs_launches", ctypes.c_uint64), ("engine", ctypes.c_int64),
+    ("solve_blocks_per_sm", ctypes.c_int64), ("relabel_work_factor", ctypes.c_double),
 ]
 
 
@@ -128,6 +129,10 @@ def lib():
                                        ctypes.POINTER(ctypes.c_uint64), p]
         L.gpupr_sample_tet_labels.argtypes = [p, p, ctypes.c_uint64, ctypes.c_int, p, ctypes.c_uint64,
                                               ctypes.c_int, p, p, f64, f64, p, ctypes.c_int, p, p]
+        L.gpupr_autotune.argtypes = [p, ctypes.c_uint64, ctypes.c_int, p, p, ctypes.c_uint64, p, ctypes.c_int,
+                                     f64, ctypes.c_int32, ctypes.c_int32, p, p]
+        L.gpupr_tune_table.argtypes = [p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+        L.gpupr_tune_table_set.argtypes = [p, ctypes.c_uint32]
         L.gpupr_release_cached_memory.argtypes = []
         L.gpupr_selftest_bounded_wait.argtypes = [ctypes.c_uint32, p]
         for name in header_functions():
@@ -452,6 +457,62 @@ def sample_tet_labels(grid, vertices, tets, bbox_min, bbox_max, padding, thresho
         float(threshold), _dp(lab) if device_out else _hp(lab), int(device_out),
         _dp(udf) if device_out else _hp(udf), _stream(torch, tets.device if t_dev else None)))
     return lab[:n], udf[:n]
+
+
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("size_class", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("work_relabel_factor", ctypes.c_double), ("solve_ms", ctypes.c_double),
+                ("default_ms", ctypes.c_double)]
+
+
+def autotune(vertices, tets, nbrs, labels, fill_T, local_steps=8, reps=3):
+    """gpupr_autotune on one cut (tets/nbrs CUDA int32): returns the chosen
+    entry of the graph's size class as a dict."""
+    import torch
+
+    v_dev = isinstance(vertices, torch.Tensor)
+    l_dev = isinstance(labels, torch.Tensor)
+    if not v_dev:
+        vertices = np.ascontiguousarray(vertices, np.float64)
+    if not l_dev:
+        labels = np.ascontiguousarray(labels, np.uint8)
+    e = TuneEntry()
+    check(lib().gpupr_autotune(_dp(vertices) if v_dev else _hp(vertices), int(vertices.shape[0]), int(v_dev),
+                               _dp(tets), _dp(nbrs), int(tets.shape[0]), _dp(labels) if l_dev else _hp(labels),
+                               int(l_dev), float(fill_T), int(local_steps), int(reps), ctypes.byref(e),
+                               _stream(torch, tets.device)))
+    return {k: getattr(e, k) for k, _ in TuneEntry._fields_}
+
+
+def tune_table():
+    n = ctypes.c_uint32(0)
+    check(lib().gpupr_tune_table(None, 0, ctypes.byref(n)))
+    arr = (TuneEntry * max(n.value, 1))()
+    check(lib().gpupr_tune_table(arr, n.value, ctypes.byref(n)))
+    return [{k: getattr(arr[i], k) for k, _ in TuneEntry._fields_} for i in range(n.value)]
+
+
+def set_tune_table(entries):
+    arr = (TuneEntry * max(len(entries), 1))()
+    for i, e in enumerate(entries):
+        for k, _ in TuneEntry._fields_:
+            setattr(arr[i], k, e.get(k, 0))
+    check(lib().gpupr_tune_table_set(arr, len(entries)))
+
+
+def save_tune_table(path):
+    """Keep the autotuned table across processes (JSON)."""
+    import json
+
+    with open(path, "w") as f:
+        json.dump(tune_table(), f, indent=1)
+
+
+def load_tune_table(path):
+    import json
+
+    with open(path) as f:
+        set_tune_table(json.load(f))
 
 
 def release_cached_memory():
