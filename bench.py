@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving loop (config 5)")
     ap.add_argument("--serve-seconds", type=float, default=8.0)
     ap.add_argument("--no-labels", action="store_true", help="skip the tet-centroid label leg")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="time the built-in grid/relabel rule instead of the autotuned table")
     ap.add_argument("--no-audit", action="store_true", help="skip the watertight audit leg")
     return ap.parse_args()
 
@@ -221,6 +223,20 @@ def run_ours(args, world, rank, local):
     import wtivo_gpupr
 
     dev = torch.device("cuda", local)
+    tune = None
+    if not args.no_autotune:
+        # the library's autotuner, run on another graph of the same generator
+        # and size (seed + 1); its table then serves the timed cuts
+        gt = make_graph(args.n_tets, args.seed + 1)
+        tt = torch.from_numpy(gt["tets"]).to(dev)
+        tn = torch.from_numpy(gt["neighbors"]).to(dev)
+        t0 = time.perf_counter()
+        tune = gpupr_capi.autotune(gt["vertices"], tt, tn, gt["labels"], 10.0, reps=3)
+        tune = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in tune.items()}
+        tune["tuning_s"] = round(time.perf_counter() - t0, 2)
+        tune["tuned_on"] = f"seed {args.seed + 1} graph of the same generator and size"
+        del gt, tt, tn
+        torch.cuda.empty_cache()
     g = make_graph(args.n_tets, args.seed)
     N = g.n_tets
     tets = torch.from_numpy(g["tets"]).to(dev)
@@ -391,9 +407,13 @@ def run_ours(args, world, rank, local):
         "solve": {"rounds": int(s0["rounds"]), "global_relabels": int(s0["global_relabels"]),
                   "bfs_levels": int(s0["bfs_levels"]), "node_visits": int(s0["node_visits"]),
                   "pushes": int(s0["pushes"]), "solve_device_ms": round(s0["solve_device_ms"], 3),
-                  "build_device_ms": round(s0["build_device_ms"], 3)},
+                  "build_device_ms": round(s0["build_device_ms"], 3),
+                  "blocks_per_sm": int(s0["solve_blocks_per_sm"]),
+                  "relabel_work_factor": float(s0["relabel_work_factor"]),
+                  "free_nodes_per_s": round(s0["free_n"] / (s0["solve_device_ms"] * 1e-3), 1),
+                  "one_sweep_floor_ms": round(60.0 * s0["free_n"] / (pk["hbm_gbs"] * 1e9) * 1e3, 4)},
         "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
-        "batch": batch, "serve": serve, "labels": labels, "audit": audit,
+        "batch": batch, "serve": serve, "labels": labels, "audit": audit, "autotune": tune,
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
     }
     return line
