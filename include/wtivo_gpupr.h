@@ -78,6 +78,8 @@ typedef struct {
     int64_t engine;             /* 1 one launch per step, 2 persistent */
     int64_t solve_blocks_per_sm;/* persistent engine: resident blocks per SM used */
     double relabel_work_factor; /* persistent engine: relabel work factor used */
+    int64_t chain_hops;         /* persistent engine: chained discharge used */
+    int64_t chain_max_active;
 } gpupr_cut_stats;
 
 /* Solver tuning knobs; zero fields take the defaults shown. */
@@ -103,6 +105,11 @@ typedef struct {
     int32_t engine;               /* 0 auto (persistent when the device supports
                                      cooperative launch), 1 one launch per BFS
                                      level / round, 2 persistent */
+    int32_t chain_hops;           /* persistent engine: nodes one thread may
+                                     discharge in a row in one round (1 = no
+                                     chaining; default 4) */
+    int32_t chain_max_active;     /* ... only in rounds with at most this many
+                                     active nodes (default 4096) */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);
@@ -382,14 +389,15 @@ gpupr_status gpupr_sample_tet_labels(const gpupr_brick_grid* grid, const double*
                                      int labels_on_device, float* udf_out, void* stream);
 
 /*
- * Autotuner (no counterpart in the reference).  The persistent engine's two
- * free choices -- resident blocks per SM and the relabel work factor -- change
- * the time of a solve, never its result.  gpupr_autotune builds the reduced
- * graph of the given cut once, then times the solve (restoring the graph each
- * time) under every pair of blocks per SM {1,2,3,4} and work factor
- * {0.5,1,2}, `reps` times each (default 3), interleaved, and keeps the pair
- * with the lowest median for the graph's size class (free nodes in
- * [2^k, 2^(k+1))).  Later solves whose options leave those fields at 0 use
+ * Autotuner (no counterpart in the reference).  The persistent engine's free
+ * choices -- resident blocks per SM, the relabel work factor and chained
+ * discharge -- change the time of a solve, never its result.  gpupr_autotune
+ * builds the reduced graph of the given cut once, then times the solve
+ * (restoring the graph each time), `reps` times each (default 3),
+ * interleaved: first every pair of blocks per SM {1,2,3,4} and work factor
+ * {0.5,1,2}, then, with the best pair, chaining off, 4 hops up to 4096 or
+ * 32768 active nodes, 8 hops up to 131072.  The setting with the lowest
+ * median is kept for the graph's size class (free nodes in [2^k, 2^(k+1))).  Later solves whose options leave those fields at 0 use
  * the table; classes without an entry keep the built-in size rule.  The
  * table is per process; gpupr_tune_table / gpupr_tune_table_set read and
  * replace it (to keep it across runs).  Arguments as gpupr_graph_cut.
@@ -398,8 +406,10 @@ typedef struct {
     int32_t size_class;           /* k: free nodes in [2^k, 2^(k+1)) */
     int32_t blocks_per_sm;
     double work_relabel_factor;
-    double solve_ms;              /* median solve time of the chosen pair */
+    double solve_ms;              /* median solve time of the chosen setting */
     double default_ms;            /* median solve time under the built-in rule */
+    int32_t chain_hops;           /* chained discharge (see gpupr_solve_options) */
+    int32_t chain_max_active;
 } gpupr_tune_entry;
 
 gpupr_status gpupr_autotune(const double* vertices, uint64_t n_vertices, int vertices_on_device,

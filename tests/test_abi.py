@@ -121,8 +121,10 @@ def test_tune_table_round_trip(built, tmp_path):
     reject invalid entries, clear."""
     import gpupr_capi
 
-    entries = [dict(size_class=18, blocks_per_sm=1, work_relabel_factor=2.0, solve_ms=10.0, default_ms=11.0),
-               dict(size_class=26, blocks_per_sm=4, work_relabel_factor=0.5, solve_ms=120.0, default_ms=130.0)]
+    entries = [dict(size_class=18, blocks_per_sm=1, work_relabel_factor=2.0, solve_ms=10.0, default_ms=11.0,
+                    chain_hops=4, chain_max_active=32768),
+               dict(size_class=26, blocks_per_sm=4, work_relabel_factor=0.5, solve_ms=120.0, default_ms=130.0,
+                    chain_hops=1, chain_max_active=1)]
     gpupr_capi.set_tune_table(entries)
     assert gpupr_capi.tune_table() == entries
     p = tmp_path / "tune.json"
@@ -132,7 +134,7 @@ def test_tune_table_round_trip(built, tmp_path):
     gpupr_capi.load_tune_table(p)
     assert gpupr_capi.tune_table() == entries
     for bad in (dict(entries[0], blocks_per_sm=0), dict(entries[0], size_class=40),
-                dict(entries[0], work_relabel_factor=0.0)):
+                dict(entries[0], work_relabel_factor=0.0), dict(entries[0], chain_hops=0)):
         with pytest.raises(gpupr_capi.GpuprError):
             gpupr_capi.set_tune_table([bad])
     assert gpupr_capi.tune_table() == entries        # a rejected set changes nothing

@@ -28,6 +28,7 @@ def test_autotune_then_cut(built):
     assert np.array_equal(out, base) and st["adjusted_flow"] == st0["adjusted_flow"]
     assert st["solve_blocks_per_sm"] == e["blocks_per_sm"]
     assert st["relabel_work_factor"] == e["work_relabel_factor"]
+    assert (st["chain_hops"], st["chain_max_active"]) == (e["chain_hops"], e["chain_max_active"])
     # explicit options still win over the table
     _, st2 = gpupr_capi.graph_cut(g["vertices"], tets, nbrs, g["labels"], g["fill_T"],
                                   opts=gpupr_capi.options(blocks_per_sm=3, work_relabel_factor=0.25))

@@ -95,7 +95,9 @@ def test_solver_invariants(built, kind, seed, size):
                                  dict(blocks_per_sm=1, round_batch=3, bfs_batch=2),
                                  dict(work_relabel_factor=0.05), dict(engine=1), dict(engine=2),
                                  dict(engine=2, blocks_per_sm=1), dict(engine=2, local_steps=1),
-                                 dict(engine=2, global_relabel_period=-1, work_relabel_factor=0.1)])
+                                 dict(engine=2, global_relabel_period=-1, work_relabel_factor=0.1),
+                                 dict(chain_hops=1), dict(chain_hops=2), dict(chain_hops=64),
+                                 dict(chain_hops=64, local_steps=1, blocks_per_sm=1)])
 def test_options_do_not_change_the_cut(built, opt):
     import gpupr_capi
 

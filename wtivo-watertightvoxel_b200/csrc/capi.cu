@@ -213,6 +213,8 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
     st->engine = sr.engine;
     st->solve_blocks_per_sm = sr.blocks_per_sm;
     st->relabel_work_factor = sr.work_factor;
+    st->chain_hops = sr.chain_hops;
+    st->chain_max_active = sr.chain_max_active;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -249,45 +251,67 @@ TuneEntry run_autotune(const double* vertices, uint64_t nv, int v_dev, const int
     struct Cand {
         int bps;
         double wf;
+        int hops, cmax;
         std::vector<double> ms;
     };
-    std::vector<Cand> cands;
-    cands.push_back({0, 0.0, {}});   // the built-in rule
-    for (int b : {1, 2, 3, 4})
-        for (double f : {0.5, 1.0, 2.0}) cands.push_back({b, f, {}});
     SolveWorkspace w;
-    for (int r = 0; r < reps; ++r)
-        for (Cand& c : cands) {
-            GPUPR_CUDA(cudaMemcpyAsync(g.res.p, res0.p, 16u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
-            GPUPR_CUDA(cudaMemcpyAsync(g.term.p, term0.p, 4u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
-            gpupr_solve_options o{};
-            o.local_steps = local_steps;
-            o.engine = 2;
-            o.blocks_per_sm = c.bps;
-            o.work_relabel_factor = c.wf;
-            SolveOptions opt = resolve_options(&o, local_steps, 1024, 2000000ull);
-            SolveResult sr;
-            solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.term.p, w, opt, s, sr);
-            c.ms.push_back(sr.solve_device_ms);
-        }
+    auto run = [&](std::vector<Cand>& cands) {
+        for (int r = 0; r < reps; ++r)
+            for (Cand& c : cands) {
+                GPUPR_CUDA(cudaMemcpyAsync(g.res.p, res0.p, 16u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+                GPUPR_CUDA(cudaMemcpyAsync(g.term.p, term0.p, 4u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+                gpupr_solve_options o{};
+                o.local_steps = local_steps;
+                o.engine = 2;
+                o.blocks_per_sm = c.bps;
+                o.work_relabel_factor = c.wf;
+                o.chain_hops = c.hops;
+                o.chain_max_active = c.cmax;
+                SolveOptions opt = resolve_options(&o, local_steps, 1024, 2000000ull);
+                SolveResult sr;
+                solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.term.p, w, opt, s, sr);
+                c.ms.push_back(sr.solve_device_ms);
+            }
+    };
     auto median = [](std::vector<double> v) {
         std::sort(v.begin(), v.end());
         return v.size() % 2 ? v[v.size() / 2] : 0.5 * (v[v.size() / 2 - 1] + v[v.size() / 2]);
     };
+    // the built-in rule (an empty table: the rule, not an older entry)
+    TuneEntry old;
+    if (tune_lookup(g.n, &old)) {
+        std::vector<TuneEntry> keep = tune_all();
+        keep.erase(std::remove_if(keep.begin(), keep.end(),
+                                  [&](const TuneEntry& e) { return e.size_class == size_class(g.n); }),
+                   keep.end());
+        tune_replace(keep);
+    }
+    // stage 1: grid x relabel schedule, default chaining
+    std::vector<Cand> c1;
+    c1.push_back({0, 0.0, 0, 0, {}});
+    for (int b : {1, 2, 3, 4})
+        for (double f : {0.5, 1.0, 2.0}) c1.push_back({b, f, 0, 0, {}});
+    run(c1);
+    const double default_ms = median(c1[0].ms);
+    size_t bi = 1;
+    for (size_t i = 2; i < c1.size(); ++i)
+        if (median(c1[i].ms) < median(c1[bi].ms)) bi = i;
+    // stage 2: chaining with the best pair
+    std::vector<Cand> c2;
+    for (auto hc : {std::pair<int, int>{1, 1}, {4, 4096}, {4, 32768}, {8, 131072}})
+        c2.push_back({c1[bi].bps, c1[bi].wf, hc.first, hc.second, {}});
+    run(c2);
+    size_t bj = 0;
+    for (size_t i = 1; i < c2.size(); ++i)
+        if (median(c2[i].ms) < median(c2[bj].ms)) bj = i;
     TuneEntry best;
     best.size_class = size_class(g.n);
-    double best_ms = 1e300;
-    for (const Cand& c : cands) {
-        if (c.bps == 0) continue;
-        const double m = median(c.ms);
-        if (m < best_ms) {
-            best_ms = m;
-            best.blocks_per_sm = c.bps;
-            best.work_factor = c.wf;
-        }
-    }
-    best.solve_ms = best_ms;
-    best.default_ms = median(cands[0].ms);
+    best.blocks_per_sm = c2[bj].bps;
+    best.work_factor = c2[bj].wf;
+    best.chain_hops = c2[bj].hops;
+    best.chain_max_active = c2[bj].cmax;
+    best.solve_ms = median(c2[bj].ms);
+    best.default_ms = default_ms;
     tune_store(best);
     return best;
 }
@@ -411,6 +435,8 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     st->engine = sr.engine;
     st->solve_blocks_per_sm = sr.blocks_per_sm;
     st->relabel_work_factor = sr.work_factor;
+    st->chain_hops = sr.chain_hops;
+    st->chain_max_active = sr.chain_max_active;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -617,6 +643,8 @@ gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_r
             stats->engine = sr.engine;
             stats->solve_blocks_per_sm = sr.blocks_per_sm;
             stats->relabel_work_factor = sr.work_factor;
+            stats->chain_hops = sr.chain_hops;
+            stats->chain_max_active = sr.chain_max_active;
             stats->kernel_launches = launches;
         }
     });
@@ -675,6 +703,8 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
             stats->engine = sr.engine;
             stats->solve_blocks_per_sm = sr.blocks_per_sm;
             stats->relabel_work_factor = sr.work_factor;
+            stats->chain_hops = sr.chain_hops;
+            stats->chain_max_active = sr.chain_max_active;
             stats->kernel_launches = launches;
         }
     });
@@ -850,6 +880,8 @@ gpupr_status gpupr_autotune(const double* vertices, uint64_t n_vertices, int ver
             chosen->work_relabel_factor = e.work_factor;
             chosen->solve_ms = e.solve_ms;
             chosen->default_ms = e.default_ms;
+            chosen->chain_hops = e.chain_hops;
+            chosen->chain_max_active = e.chain_max_active;
         }
     });
 }
@@ -866,6 +898,8 @@ gpupr_status gpupr_tune_table(gpupr_tune_entry* entries, uint32_t capacity, uint
             entries[i].work_relabel_factor = all[i].work_factor;
             entries[i].solve_ms = all[i].solve_ms;
             entries[i].default_ms = all[i].default_ms;
+            entries[i].chain_hops = all[i].chain_hops;
+            entries[i].chain_max_active = all[i].chain_max_active;
         }
     });
 }
@@ -881,6 +915,8 @@ gpupr_status gpupr_tune_table_set(const gpupr_tune_entry* entries, uint32_t coun
             v[i].work_factor = entries[i].work_relabel_factor;
             v[i].solve_ms = entries[i].solve_ms;
             v[i].default_ms = entries[i].default_ms;
+            v[i].chain_hops = entries[i].chain_hops;
+            v[i].chain_max_active = entries[i].chain_max_active;
         }
         tune_replace(v);
     });

@@ -57,6 +57,9 @@ struct SolveView {
     uint32_t* fr[2];                    // BFS frontiers (fr[1] aliases act[1])
     Ctl* ctl;
     int local_steps;
+    int chain_hops;                     // nodes one thread may discharge in a row in
+                                        // one round (<= 1: no chaining) ...
+    uint32_t chain_max_active;          // ... in rounds of at most this many nodes
 };
 
 // ---------------------------------------------------------------------------
@@ -209,6 +212,8 @@ struct SolveOptions {
     int blocks_per_sm = 0;         // 0: by graph size (persistent), 4 (one launch per step)
     double work_factor = 0.0;      // node visits per node between relabels, 0 = engine default
     int engine = 0;                // 0 auto, 1 one launch per step, 2 persistent
+    int chain_hops = 0;            // persistent engine: 0 = default
+    int chain_max_active = 0;      // persistent engine: 0 = default
 };
 
 SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw,
@@ -236,6 +241,7 @@ struct SolveResult {
     int engine = 1;                // 1 one launch per step, 2 persistent
     int blocks_per_sm = 0;         // persistent engine: grid used
     double work_factor = 0.0;      // persistent engine: relabel work factor used
+    int chain_hops = 0, chain_max_active = 0;   // persistent engine: chaining used
 };
 
 // Autotuner table (push_relabel.cu): per size class (floor(log2 n)), the
@@ -243,6 +249,7 @@ struct SolveResult {
 struct TuneEntry {
     int32_t size_class = 0, blocks_per_sm = 0;
     double work_factor = 0.0, solve_ms = 0.0, default_ms = 0.0;
+    int32_t chain_hops = 4, chain_max_active = 4096;
 };
 bool tune_lookup(uint32_t n, TuneEntry* out);
 void tune_store(const TuneEntry& e);

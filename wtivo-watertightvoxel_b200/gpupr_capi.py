@@ -36,6 +36,7 @@ STATS_FIELDS = [
     ("bfs_ms", ctypes.c_double), ("discharge_launches", ctypes.c_uint64),
     ("bfs_launches", ctypes.c_uint64), ("engine", ctypes.c_int64),
     ("solve_blocks_per_sm", ctypes.c_int64), ("relabel_work_factor", ctypes.c_double),
+    ("chain_hops", ctypes.c_int64), ("chain_max_active", ctypes.c_int64),
 ]
 
 
@@ -53,6 +54,7 @@ class SolveOptions(ctypes.Structure):
         ("round_batch", ctypes.c_int32), ("bfs_batch", ctypes.c_int32),
         ("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
         ("work_relabel_factor", ctypes.c_double), ("engine", ctypes.c_int32),
+        ("chain_hops", ctypes.c_int32), ("chain_max_active", ctypes.c_int32),
     ]
 
 
@@ -462,7 +464,8 @@ def sample_tet_labels(grid, vertices, tets, bbox_min, bbox_max, padding, thresho
 class TuneEntry(ctypes.Structure):
     _fields_ = [("size_class", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
                 ("work_relabel_factor", ctypes.c_double), ("solve_ms", ctypes.c_double),
-                ("default_ms", ctypes.c_double)]
+                ("default_ms", ctypes.c_double), ("chain_hops", ctypes.c_int32),
+                ("chain_max_active", ctypes.c_int32)]
 
 
 def autotune(vertices, tets, nbrs, labels, fill_T, local_steps=8, reps=3):
