@@ -75,3 +75,31 @@ def test_destroy_finishes_submitted_requests(built):
     sv.close()                          # returns only after every request is cut
     for out, lab in zip(outs, want):
         assert np.array_equal(out[:len(lab)], lab)
+
+
+def test_bad_request_does_not_fail_its_batch(built):
+    """A request with a neighbor id outside its graph fails alone, with the
+    reference's message; the requests batched with it get their cuts."""
+    import gpupr_capi
+
+    pool = _pool()
+    want = [orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0) for g in pool]
+    bad = dict(pool[1])
+    bad["neighbors"] = pool[1]["neighbors"].copy()
+    i = int(np.nonzero((bad["neighbors"] >= 0).all(1))[0][0])
+    bad["neighbors"][i, 0] = len(pool[1]["tets"]) + 9
+    with gpupr_capi.Server() as sv:
+        # a slow first request lets the rest pile up into one batch
+        big = cached_graph("lattice", 2, 80_000)
+        first = sv.submit(big["vertices"], big["tets"], big["neighbors"], big["labels"])
+        ids = [sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"]) for g in pool[:1]]
+        bad_id = sv.submit(bad["vertices"], bad["tets"], bad["neighbors"], bad["labels"])
+        ids += [sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"]) for g in pool[2:]]
+        sv.wait(first, timeout_s=120)
+        with pytest.raises(gpupr_capi.GpuprError, match="neighbor out of range"):
+            sv.wait(bad_id, timeout_s=120)
+        for rid, gi in zip(ids, [0, 2, 3]):
+            out, res = sv.wait(rid, timeout_s=120)
+            lab, st = want[gi]
+            assert res["status"] == 0 and np.array_equal(out, lab)
+            assert res["adjusted_flow"] == st["adjusted_flow"]

@@ -28,6 +28,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -48,6 +49,7 @@ struct gpupr_server {
         Clock::time_point t_submit, t_start;
         bool done = false;
         gpupr_status status = GPUPR_OK;
+        std::string error;              // the failure's message, when status != OK
         gpupr_request_result result{};
     };
     struct Batch {
@@ -90,7 +92,11 @@ struct gpupr_server {
     void solve_loop();
     void upload(Batch& b);
     void solve(Batch& b);
-    void publish(Batch& b, const std::vector<gpupr_batch_item>* items, Clock::time_point t_done);
+    // results of a batch: per-request items/status/message when given, else
+    // the batch's status for every request
+    void publish(Batch& b, const std::vector<gpupr_batch_item>* items,
+                 const std::vector<gpupr_status>* status, const std::vector<std::string>* msg,
+                 Clock::time_point t_done);
 };
 
 void gpupr_server::upload(Batch& b)
@@ -126,37 +132,68 @@ void gpupr_server::solve(Batch& b)
 {
     using namespace gpupr;
     const uint32_t G = (uint32_t)b.reqs.size();
-    const uint64_t N = b.toff[G];
     std::vector<gpupr_batch_item> items(G);
-    gpupr_cut_stats st{};
-    try {
+    std::vector<gpupr_status> status(G, GPUPR_OK);
+    std::vector<std::string> msg(G);
+    // cuts requests [k0, k0 + cnt) as one batch; labels straight to their callers
+    auto cut = [&](uint32_t k0, uint32_t cnt) {
+        std::vector<uint64_t> toff(cnt + 1), voff(cnt + 1);
+        for (uint32_t k = 0; k <= cnt; ++k) {
+            toff[k] = b.toff[k0 + k] - b.toff[k0];
+            voff[k] = b.voff[k0 + k] - b.voff[k0];
+        }
+        const uint64_t N = toff[cnt];
+        gpupr_cut_stats st{};
         DevBuf<uint8_t> dout(N, run);
-        run_graph_cut_batch(G, b.toff.data(), b.voff.data(), b.dV.p, 1, b.dT.p, b.dN.p, b.dL.p, 1,
-                            b.reqs[0]->fill_T, has_opts ? &opts : nullptr, dout.p, 1, run,
-                            items.data(), &st);
-        for (uint32_t k = 0; k < G; ++k)
-            device_to_host(b.reqs[k]->out, dout.p + b.toff[k], b.reqs[k]->n, run);
+        run_graph_cut_batch(cnt, toff.data(), voff.data(), b.dV.p + b.voff[k0] * 3u, 1,
+                            b.dT.p + b.toff[k0] * 4u, b.dN.p + b.toff[k0] * 4u, b.dL.p + b.toff[k0], 1,
+                            b.reqs[k0]->fill_T, has_opts ? &opts : nullptr, dout.p, 1, run,
+                            items.data() + k0, &st);
+        for (uint32_t k = 0; k < cnt; ++k)
+            device_to_host(b.reqs[k0 + k]->out, dout.p + toff[k], b.reqs[k0 + k]->n, run);
         GPUPR_CUDA(cudaStreamSynchronize(run));
-    } catch (const Error& e) {
-        b.status = e.status;
+    };
+    auto guarded_cut = [&](uint32_t k0, uint32_t cnt) -> bool {
+        gpupr_status s0 = GPUPR_OK;
+        std::string m;
+        try {
+            cut(k0, cnt);
+            return true;
+        } catch (const Error& e) {
+            s0 = e.status;
+            m = e.msg;
+        } catch (...) {
+            s0 = GPUPR_ERR_CUDA;
+            m = "unknown failure";
+        }
         cudaStreamSynchronize(run);
         cudaGetLastError();
-    } catch (...) {
-        b.status = GPUPR_ERR_CUDA;
-        cudaStreamSynchronize(run);
-        cudaGetLastError();
-    }
+        for (uint32_t k = k0; k < k0 + cnt; ++k) {
+            status[k] = s0;
+            msg[k] = m;
+        }
+        return false;
+    };
+    // one bad request must not fail the others: when the batch fails, every
+    // request is cut alone and keeps its own result or error
+    if (!guarded_cut(0, G) && G > 1)
+        for (uint32_t k = 0; k < G; ++k) {
+            status[k] = GPUPR_OK;
+            msg[k].clear();
+            guarded_cut(k, 1);
+        }
     // the staged buffers were written on the upload stream and read on this
     // one, whose work is complete: release them now
     b.dT.reset();
     b.dN.reset();
     b.dL.reset();
     b.dV.reset();
-    publish(b, b.status == GPUPR_OK ? &items : nullptr, Clock::now());
+    publish(b, &items, &status, &msg, Clock::now());
 }
 
 void gpupr_server::publish(Batch& b, const std::vector<gpupr_batch_item>* items,
-                           Clock::time_point t_done)
+                           const std::vector<gpupr_status>* status,
+                           const std::vector<std::string>* msg, Clock::time_point t_done)
 {
     const uint32_t G = (uint32_t)b.reqs.size();
     auto ms = [](Clock::time_point a, Clock::time_point z) {
@@ -165,14 +202,15 @@ void gpupr_server::publish(Batch& b, const std::vector<gpupr_batch_item>* items,
     std::lock_guard<std::mutex> lk(mu);
     for (uint32_t k = 0; k < G; ++k) {
         auto& r = *b.reqs[k];
-        r.status = b.status;
-        if (items) {
+        r.status = status ? (*status)[k] : b.status;
+        if (r.status != GPUPR_OK) r.error = msg ? (*msg)[k] : std::string(gpupr_status_string(r.status));
+        if (items && r.status == GPUPR_OK) {
             r.result.adjusted_flow = (*items)[k].adjusted_flow;
             r.result.raw_flow = (*items)[k].raw_flow;
             r.result.free_n = (*items)[k].free_n;
         }
         r.result.id = r.id;
-        r.result.status = b.status;
+        r.result.status = r.status;
         r.result.n_tets = r.n;
         r.result.batch_size = (int32_t)G;
         r.result.queue_ms = ms(r.t_submit, r.t_start);
@@ -233,7 +271,7 @@ void gpupr_server::stage_loop()
             b->dN.reset();
             b->dL.reset();
             b->dV.reset();
-            publish(*b, nullptr, Clock::now());
+            publish(*b, nullptr, nullptr, nullptr, Clock::now());
             continue;
         }
         std::lock_guard<std::mutex> lk(mu);
@@ -350,7 +388,7 @@ gpupr_status gpupr_server_wait(gpupr_server* sv, uint64_t request_id, double tim
         gpupr::set_last_error("request not finished within the timeout");
         return GPUPR_ERR_TIMEOUT;
     }
-    if (r->status != GPUPR_OK) gpupr::set_last_error(gpupr_status_string(r->status));
+    if (r->status != GPUPR_OK) gpupr::set_last_error(r->error);
     if (result) *result = r->result;
     sv->all.erase(it);   // the result is read out: release it
     return r->status;
