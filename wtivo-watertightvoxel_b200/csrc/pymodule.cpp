@@ -23,6 +23,8 @@
 #include <stdexcept>
 #include <string>
 
+#include <sys/mman.h>
+
 #include "wtivo_gpupr.h"
 
 namespace py = pybind11;
@@ -85,6 +87,23 @@ void* current_stream(int device)
 }
 
 using F64 = py::array_t<double, py::array::c_style | py::array::forcecast>;
+
+// The returned labels (one byte per tet, 80 MB at benchmark size) in memory
+// aligned to 2 MiB and advised for huge pages: the copy from the device then
+// touches a few dozen pages instead of ~20,000 fresh 4 KiB ones.  A plain
+// numpy array owns it through a capsule.
+py::array_t<std::uint8_t> label_array(std::uint64_t n)
+{
+    const std::size_t huge = 2u << 20;
+    if (n < 2 * huge) return py::array_t<std::uint8_t>(static_cast<py::ssize_t>(n));
+    const std::size_t bytes = (static_cast<std::size_t>(n) + huge - 1) / huge * huge;
+    void* p = nullptr;
+    if (posix_memalign(&p, huge, bytes) != 0 || !p) throw std::bad_alloc();
+    madvise(p, bytes, MADV_HUGEPAGE);   // advice only: ignored where unsupported
+    py::capsule owner(p, [](void* q) { std::free(q); });
+    return py::array_t<std::uint8_t>({static_cast<py::ssize_t>(n)}, {static_cast<py::ssize_t>(1)},
+                                     static_cast<std::uint8_t*>(p), owner);
+}
 using U8 = py::array_t<std::uint8_t, py::array::c_style | py::array::forcecast>;
 
 py::tuple graph_cut_fast(F64 vertices, py::object tets_cuda, py::object nbr_cuda, U8 labels,
@@ -101,7 +120,7 @@ py::tuple graph_cut_fast(F64 vertices, py::object tets_cuda, py::object nbr_cuda
     if (N > 0xFFFFFFFFull) throw std::runtime_error(">2^32 full tets unsupported");
     const std::uint64_t nv = static_cast<std::uint64_t>(vertices.shape(0));
     void* stream = current_stream(t.device);
-    py::array_t<std::uint8_t> out(static_cast<py::ssize_t>(N));
+    py::array_t<std::uint8_t> out = label_array(N);
     gpupr_cut_stats st{};
     gpupr_status rc;
     {
