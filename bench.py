@@ -14,8 +14,14 @@ reference's 12M-point CGAL Delaunay), lambda_fill = 10.
 * ``e2e``: the same metric through the drop-in ``wtivo_gpupr.graph_cut_fast``
   with host vertices/labels, tets/neighbors copied from pinned host memory
   every step, and the labels read back.
-* ``roofline``: the dominant solver phase (CUDA events around its launch
-  batches, live in this run) against the measured HBM copy bandwidth.
+* ``roofline``: the dominant kernel (the persistent solver: one launch per
+  cut, CUDA events around it, live in this run) by algorithmic bytes against
+  the measured HBM copy bandwidth; its DRAM traffic from an ncu capture; for
+  context, the rate at which this GPU serves independent random 4-byte reads.
+* ``batch`` / ``serve`` / ``labels`` / ``audit`` / ``autotune``: the batched
+  cut of 64 uneven graphs, the serving loop under Poisson arrivals, the
+  tet-centroid label sampler, the watertight audit of the cut surface, and
+  the autotuner's choice (tuned on another graph of the same generator).
 * ``cpu_baseline``: the CPU oracle (single-threaded Boykov-Kolmogorov, with
   the reference's graph reduction) on a bounded sample of the same workload.
 * ``--impl reference``: the reference's own module (compiled from its
@@ -48,7 +54,7 @@ for _p in (str(PKG), str(ROOT)):
 METRIC = "cut solve tets/s (12M-pt-scale graph, ~80M tets, 1 B200)"
 WORKLOAD = "torus-knot (3,5) tube, 2% patches dropped, inner shell 0.002, noise 1e-4; Kuhn lattice ~80M tets; lambda_fill=10"
 
-# algorithmic bytes per unit ("Roofline"): discharge node visit
+# algorithmic bytes per unit of the solver: a discharge node visit
 # reads nbr 16 + res 16 + rev 1 + term 4 + excess 8 + height 4 + 4 neighbour
 # heights 16, queue read+write 8 = 73 B; each push adds res+reverse res 8 and
 # two excess updates 16 = 24 B; a BFS frontier expansion reads nbr 16 + rev 1
@@ -304,6 +310,13 @@ def run_ours(args, world, rank, local):
                 "engine": int(stats[-1]["engine"]),
                 "phase_ms_per_step": {"solve": round(sum(s["solve_device_ms"] for s in stats) / args.steps, 3),
                                       "build": round(sum(s["build_device_ms"] for s in stats) / args.steps, 3)}}
+    if rank == 0:
+        rs = random_sector_rate(dev)
+        roofline["random_sector_gbs"] = round(rs, 1)
+        if isinstance(traffic, (int, float)) and kms > 0:
+            dram = traffic / (kms / max(launches, 1) * 1e-3) / 1e9
+            roofline["traffic_gbs"] = round(dram, 1)
+            roofline["traffic_frac_of_random_sector_rate"] = round(dram / rs, 4)
 
     # e2e through the drop-in module: pinned host topology, host V/labels
     e2e = None
@@ -431,6 +444,23 @@ def cuda_ms(fn, reps, stream):
     b.record(stream)
     torch.cuda.synchronize()
     return a.elapsed_time(b) / reps
+
+
+def random_sector_rate(dev):
+    """Context for the solver's roofline: the rate at which this GPU serves
+    independent random 4-byte reads from a 2 GiB array (each moves one 32-byte
+    sector), measured with torch's gather (a library kernel) as GB/s of
+    sectors.  The solver's accesses are of that kind."""
+    import torch
+
+    src = torch.empty(1 << 29, dtype=torch.float32, device=dev)
+    idx = torch.randint(0, 1 << 29, (1 << 26,), device=dev)
+    for _ in range(2):
+        torch.index_select(src, 0, idx)
+    ms = cuda_ms(lambda: torch.index_select(src, 0, idx), 5, torch.cuda.current_stream(dev))
+    del src, idx
+    torch.cuda.empty_cache()
+    return (1 << 26) * 32 / (ms * 1e-3) / 1e9
 
 
 def run_labels(args, local, g):
