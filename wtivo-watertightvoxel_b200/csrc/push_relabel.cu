@@ -734,14 +734,17 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     GPUPR_CUDA(cudaEventRecord(e0, s));
     SolveView gv = g;
     // Chained discharge pays where a round is a latency chain (few active
-    // nodes) and can multiply node visits in wide rounds; how wide depends on
-    // the graph (measured on B200, 4 hops: 32768 active nodes took a 277k-node
-    // graph from 13.9 to 8.4 ms and a 2.9M-node one from 6.6 to 10.0 ms;
-    // 4096 gave 10.8 and 6.6), so the default is the safe 4096 and the
-    // autotuner may pick another.
+    // nodes) and can multiply node visits in wide rounds.  Measured on B200
+    // with 4 hops over 18 graphs below 1.5M free nodes: chaining in rounds of
+    // up to 131072 active nodes took 59.5 ms in all against 69.8 ms with
+    // 4096; between 1.5M and 2M, 32768 was best; above, only 4096 did not
+    // slow any graph down (a 2.9M-node torus: 6.6 ms, 10.0 with 32768).  The
+    // autotuner may pick another setting.
     gv.chain_hops = opt.chain_hops > 0 ? opt.chain_hops : tuned ? te.chain_hops : 4;
     gv.chain_max_active = opt.chain_max_active > 0 ? (uint32_t)opt.chain_max_active
                           : tuned                  ? (uint32_t)te.chain_max_active
+                          : g.n < 1500000u         ? 131072u
+                          : g.n < 2000000u         ? 32768u
                                                    : 4096u;
     void* args[] = {&gv, &p};
     GPUPR_CUDA(cudaLaunchCooperativeKernel((const void*)k_solve_persistent, dim3(grid), dim3(DTPB),
