@@ -100,8 +100,8 @@ typedef struct {
                                      (persistent) */
     double work_relabel_factor;   /* relabel after this many node visits per
                                      free node since the last one; default 3
-                                     (one launch per step), 2 below 500k free
-                                     nodes else 1 (persistent) */
+                                     (one launch per step); persistent: 2 below
+                                     500k free nodes, 1 below 10M, else 0.5 */
     int32_t engine;               /* 0 auto (persistent when the device supports
                                      cooperative launch), 1 one launch per BFS
                                      level / round, 2 persistent */
@@ -398,8 +398,9 @@ gpupr_status gpupr_sample_tet_labels(const gpupr_brick_grid* grid, const double*
  * (restoring the graph each time), `reps` times each (default 3),
  * interleaved: first every pair of blocks per SM {1,2,3,4} and work factor
  * {0.5,1,2}, then, with the best pair, chaining off, 4 hops up to 4096 or
- * 32768 active nodes, 8 hops up to 131072.  The setting with the lowest
- * median is kept for the graph's size class (free nodes in [2^k, 2^(k+1))).  Later solves whose options leave those fields at 0 use
+ * 32768 active nodes, 8 hops up to 131072, beside the built-in rule.  The
+ * setting with the lowest median (the rule's own values when it wins) is
+ * kept for the graph's size class (free nodes in [2^k, 2^(k+1))).  Later solves whose options leave those fields at 0 use
  * the table; classes without an entry keep the built-in size rule.  The
  * table is per process; gpupr_tune_table / gpupr_tune_table_set read and
  * replace it (to keep it across runs).  Arguments as gpupr_graph_cut.

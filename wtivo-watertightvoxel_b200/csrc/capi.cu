@@ -253,6 +253,7 @@ TuneEntry run_autotune(const double* vertices, uint64_t nv, int v_dev, const int
         double wf;
         int hops, cmax;
         std::vector<double> ms;
+        SolveResult last;   // settings the solve actually used
     };
     SolveWorkspace w;
     auto run = [&](std::vector<Cand>& cands) {
@@ -271,6 +272,7 @@ TuneEntry run_autotune(const double* vertices, uint64_t nv, int v_dev, const int
                 SolveResult sr;
                 solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.term.p, w, opt, s, sr);
                 c.ms.push_back(sr.solve_device_ms);
+                c.last = sr;
             }
     };
     auto median = [](std::vector<double> v) {
@@ -288,30 +290,34 @@ TuneEntry run_autotune(const double* vertices, uint64_t nv, int v_dev, const int
     }
     // stage 1: grid x relabel schedule, default chaining
     std::vector<Cand> c1;
-    c1.push_back({0, 0.0, 0, 0, {}});
+    c1.push_back({0, 0.0, 0, 0, {}, {}});
     for (int b : {1, 2, 3, 4})
-        for (double f : {0.5, 1.0, 2.0}) c1.push_back({b, f, 0, 0, {}});
+        for (double f : {0.5, 1.0, 2.0}) c1.push_back({b, f, 0, 0, {}, {}});
     run(c1);
-    const double default_ms = median(c1[0].ms);
     size_t bi = 1;
     for (size_t i = 2; i < c1.size(); ++i)
         if (median(c1[i].ms) < median(c1[bi].ms)) bi = i;
-    // stage 2: chaining with the best pair
+    // stage 2: chaining with the best pair, against the built-in rule again:
+    // the entry never replaces the rule by a setting that was not faster
     std::vector<Cand> c2;
+    c2.push_back({0, 0.0, 0, 0, {}, {}});
     for (auto hc : {std::pair<int, int>{1, 1}, {4, 4096}, {4, 32768}, {8, 131072}})
-        c2.push_back({c1[bi].bps, c1[bi].wf, hc.first, hc.second, {}});
+        c2.push_back({c1[bi].bps, c1[bi].wf, hc.first, hc.second, {}, {}});
     run(c2);
     size_t bj = 0;
     for (size_t i = 1; i < c2.size(); ++i)
         if (median(c2[i].ms) < median(c2[bj].ms)) bj = i;
+    const Cand& win = c2[bj];
     TuneEntry best;
     best.size_class = size_class(g.n);
-    best.blocks_per_sm = c2[bj].bps;
-    best.work_factor = c2[bj].wf;
-    best.chain_hops = c2[bj].hops;
-    best.chain_max_active = c2[bj].cmax;
-    best.solve_ms = median(c2[bj].ms);
-    best.default_ms = default_ms;
+    best.blocks_per_sm = win.bps ? win.bps : win.last.blocks_per_sm;
+    best.work_factor = win.wf > 0 ? win.wf : win.last.work_factor;
+    best.chain_hops = win.hops ? win.hops : win.last.chain_hops;
+    best.chain_max_active = win.cmax ? win.cmax : win.last.chain_max_active;
+    best.solve_ms = median(win.ms);
+    std::vector<double> dflt = c1[0].ms;
+    dflt.insert(dflt.end(), c2[0].ms.begin(), c2[0].ms.end());
+    best.default_ms = median(dflt);
     tune_store(best);
     return best;
 }
