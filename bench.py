@@ -18,10 +18,11 @@ reference's 12M-point CGAL Delaunay), lambda_fill = 10.
   cut, CUDA events around it, live in this run) by algorithmic bytes against
   the measured HBM copy bandwidth; its DRAM traffic from an ncu capture; for
   context, the rate at which this GPU serves independent random 4-byte reads.
-* ``batch`` / ``serve`` / ``labels`` / ``audit`` / ``autotune``: the batched
-  cut of 64 uneven graphs, the serving loop under Poisson arrivals, the
-  tet-centroid label sampler, the watertight audit of the cut surface, and
-  the autotuner's choice (tuned on another graph of the same generator).
+* ``batch`` / ``serve`` / ``labels`` / ``audit`` / ``raw`` / ``autotune``: the
+  batched cut of 64 uneven graphs, the serving loop under Poisson arrivals,
+  the tet-centroid label sampler, the watertight audit of the cut surface, a
+  raw integer graph through gpupr_solve_ell, and the autotuner's choice
+  (tuned on another graph of the same generator).
 * ``cpu_baseline``: the CPU oracle (single-threaded Boykov-Kolmogorov, with
   the reference's graph reduction) on a bounded sample of the same workload.
 * ``--impl reference``: the reference's own module (compiled from its
@@ -80,6 +81,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true",
                     help="time the built-in grid/relabel rule instead of the autotuned table")
     ap.add_argument("--no-audit", action="store_true", help="skip the watertight audit leg")
+    ap.add_argument("--no-raw", action="store_true", help="skip the raw integer graph leg (config 4)")
     return ap.parse_args()
 
 
@@ -404,6 +406,7 @@ def run_ours(args, world, rank, local):
     serve = run_serve(args) if rank == 0 and not args.no_serve else None
     labels = run_labels(args, local, g) if rank == 0 and not args.no_labels else None
     audit = run_audit(args, local, g, out, tets, nbrs) if rank == 0 and not args.no_audit else None
+    raw = run_raw(args, local) if rank == 0 and not args.no_raw else None
 
     s0 = stats[-1]
     line = {
@@ -426,7 +429,7 @@ def run_ours(args, world, rank, local):
                   "free_nodes_per_s": round(s0["free_n"] / (s0["solve_device_ms"] * 1e-3), 1),
                   "one_sweep_floor_ms": round(60.0 * s0["free_n"] / (pk["hbm_gbs"] * 1e9) * 1e3, 4)},
         "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
-        "batch": batch, "serve": serve, "labels": labels, "audit": audit, "autotune": tune,
+        "batch": batch, "serve": serve, "labels": labels, "audit": audit, "raw": raw, "autotune": tune,
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
     }
     return line
@@ -518,6 +521,52 @@ def run_labels(args, local, g):
                          "peak_source": pk_kind, "algorithmic_bytes": int(alg)},
             "cpu_baseline": {"value": round(n_cpu / cpu_s, 1), "unit": "tets/s", "cores": 1, "kind": "port",
                              "sample": f"first {n_cpu} tets, oracle/wtivo_oracle.c"}}
+
+
+def run_raw(args, local):
+    """Config 4: a raw integer graph (all nodes free, given integer n-links
+    and t-links; gpupr_solve_ell) of 11.7M nodes (125^3-cube Kuhn lattice over
+    uniform space, area-proportional n-links, noisy sphere-SDF t-links),
+    inputs in HBM; checked by the max-flow = min-cut identity; CPU baseline:
+    the BK oracle, 1 core, on the 1.4M-node graph of the same generator."""
+    import torch
+
+    import gpupr_capi
+    import synth
+    from oracle import oracle as orc
+
+    dev = torch.device("cuda", local)
+    g = synth.config4(args.seed, n_points=2_000_000, use_delaunay=False)
+    nbr, cap, s, k = (torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+                      for x in (g["nbr"], g["cap"].view(np.int32), g["src"].view(np.int32),
+                                g["snk"].view(np.int32)))
+    n = int(nbr.shape[0])
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        flow, part, st = gpupr_capi.solve_ell(nbr, cap, s, k)
+    ms = cuda_ms(lambda: gpupr_capi.solve_ell(nbr, cap, s, k), 5, stream)
+    # certificate: capacity of the returned cut in the input graph
+    p = part.long()
+    valid = nbr >= 0
+    pu = torch.where(valid, p[nbr.long().clamp_min(0)], torch.zeros_like(nbr).long())
+    nl = (cap.long() * (valid & (p[:, None] == 0) & (pu == 1))).sum()
+    src, snk = s.long(), k.long()
+    cut = int((nl + torch.where(p == 0, snk, torch.zeros_like(snk)).sum()
+               + torch.where(p == 1, src, torch.zeros_like(src)).sum()).item())
+    gs = synth.config4(args.seed, n_points=250_000, use_delaunay=False)
+    term = (gs["src"].astype(np.int64) - gs["snk"].astype(np.int64)).astype(np.int32)
+    t0 = time.perf_counter()
+    orc.maxflow_bk(gs["nbr"], gs["cap"], term)
+    cpu_s = time.perf_counter() - t0
+    return {"config": "raw integer graph, 125^3-cube Kuhn lattice (11.7M nodes), integer n-links "
+                      "round(1e4 area/mean), sphere-SDF t-links, inputs in HBM",
+            "nodes": n, "flow": int(flow), "cut_capacity_equals_flow": bool(cut == flow),
+            "ms": round(ms, 3), "nodes_per_s": round(n / (ms * 1e-3), 1),
+            "solve_device_ms": round(st["solve_device_ms"], 3), "rounds": int(st["rounds"]),
+            "global_relabels": int(st["global_relabels"]),
+            "cpu_baseline": {"value": round(len(gs["nbr"]) / cpu_s, 1), "unit": "nodes/s", "cores": 1,
+                             "kind": "port", "sample": f"{len(gs['nbr'])}-node graph of the same "
+                                                       "generator, BK max flow, oracle/wtivo_oracle.c"}}
 
 
 def run_audit(args, local, g, labels_dev, tets, nbrs):
