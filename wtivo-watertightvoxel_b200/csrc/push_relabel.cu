@@ -4,9 +4,14 @@
 // Replaces cellocut_gpu_push_relabel_fast
 // (native/gpupr/gpu_push_relabel_fast.cu:406-571).  Differences in design:
 //
-//  * No host round trip per round or per BFS level: kernels read their
-//    queue sizes from a device control block (ring counters), and the host
-//    enqueues batches of rounds/levels and checks the state once per batch.
+//  * No host round trip per round or per BFS level.  The default engine is
+//    one persistent cooperative kernel (k_solve_persistent) that runs the
+//    whole solve, steps separated by a bounded software grid barrier; the
+//    other engine launches one kernel per step, reading queue sizes from a
+//    device control block (ring counters), with the host checking the state
+//    once per batch of steps.
+//  * Chained discharge: the thread that takes ownership of a neighbour's
+//    excess may discharge it at once, so excess moves several hops a round.
 //  * Reverse slots are precomputed at build time (2 bits per slot), so a push
 //    or a BFS step never searches the neighbor's row (.cu:56-67).
 //  * Queue de-duplication without flags: a node owns its excess; the thread
