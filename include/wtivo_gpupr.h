@@ -20,7 +20,8 @@
 extern "C" {
 #endif
 
-#define GPUPR_ABI_VERSION 1
+#define GPUPR_ABI_VERSION 2   /* 2: stats and options carry the persistent engine's
+                                 grid, relabel factor and chaining; tuning entries */
 
 typedef enum {
     GPUPR_OK = 0,
