@@ -94,21 +94,40 @@ __global__ void __launch_bounds__(DTPB) k_init_excess(uint32_t n, const int32_t*
 // Frontier size up to which a BFS level loads every neighbor's state at once.
 constexpr uint32_t BFS_EAGER_MAX = 32768u;
 
+// Nodes per thread in the whole-array passes (BFS seed, excess init): that
+// many independent loads in flight per thread make the pass stream instead
+// of waiting for one round trip per node.
+constexpr int SWEEP_UNROLL = 4;
+
 // Level 1 of the backward BFS: nodes with a residual arc to the sink.  Every
 // other height is reset to UNVIS (.cu:374-379).  s_m[0..5] are the block's
-// staging counters (frontier count, active count, and their flush copies).
+// staging counters (frontier count, active count, and their flush copies);
+// s_fr and s_act hold DTPB * SWEEP_UNROLL entries each.
 __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr, uint32_t* s_act,
                                               uint32_t* s_m)
 {
     Ctl* ctl = g.ctl;
-    for (uint32_t base = blockIdx.x * DTPB; base < g.n; base += gridDim.x * DTPB) {
-        const uint32_t v = base + threadIdx.x;
-        if (v < g.n) {
-            const int32_t t = ldcg(g.term + v);
-            g.height[v] = (t < 0) ? 1u : UNVIS;
-            if (t < 0) {
+    constexpr uint32_t CH = DTPB * SWEEP_UNROLL;
+    for (uint32_t base = blockIdx.x * CH; base < g.n; base += gridDim.x * CH) {
+        int32_t t[SWEEP_UNROLL];
+#pragma unroll
+        for (int j = 0; j < SWEEP_UNROLL; ++j) {
+            const uint32_t v = base + j * DTPB + threadIdx.x;
+            t[j] = v < g.n ? ldcg(g.term + v) : 0;
+        }
+        long long x[SWEEP_UNROLL];
+#pragma unroll
+        for (int j = 0; j < SWEEP_UNROLL; ++j) {
+            const uint32_t v = base + j * DTPB + threadIdx.x;
+            x[j] = (v < g.n && t[j] < 0) ? ldcg(g.excess + v) : 0ll;
+            if (v < g.n) g.height[v] = (t[j] < 0) ? 1u : UNVIS;
+        }
+#pragma unroll
+        for (int j = 0; j < SWEEP_UNROLL; ++j) {
+            const uint32_t v = base + j * DTPB + threadIdx.x;
+            if (v < g.n && t[j] < 0) {
                 s_fr[atomicAdd(&s_m[0], 1u)] = v;
-                if (1u < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_m[1], 1u)] = v;
+                if (1u < g.n && x[j] > 0) s_act[atomicAdd(&s_m[1], 1u)] = v;
             }
         }
         __syncthreads();
@@ -124,13 +143,46 @@ __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr
     }
 }
 
+// Queues up to this size are spread over every SM (queue_index).
+constexpr uint32_t SPREAD_MAX = 65536u;
+
+// Queue index of a thread's entry in pass `it` over a queue of cnt entries;
+// pass `it` covers indices [it * gridDim.x * DTPB, (it + 1) * gridDim.x * DTPB).
+// A short queue (cnt <= SPREAD_MAX) is dealt to warps in 32-entry chunks
+// round-robin over the blocks, so it is spread over every SM; measured on
+// B200, a BFS level of 2-4K nodes on the first 8-16 blocks (12 random loads
+// per node in flight, thousands per SM) took ~9.7 us, spread ~7.5 us.  A long
+// queue keeps 256 consecutive entries per block: they were appended by one
+// block of the step before and are near each other in the graph, and the
+// spread order made levels of 262K+ nodes 15% slower.
+__device__ __forceinline__ uint32_t queue_index(uint32_t it, uint32_t cnt)
+{
+    if (cnt <= SPREAD_MAX) {
+        const uint32_t chunk = (it * (DTPB / 32) + (threadIdx.x >> 5)) * gridDim.x + blockIdx.x;
+        return chunk * 32u + (threadIdx.x & 31u);
+    }
+    return (it * gridDim.x + blockIdx.x) * DTPB + threadIdx.x;
+}
+
+// A thread's first entry of a short queue (queue_index(0, cnt <= SPREAD_MAX)),
+// loaded by an L2 load that stays in program order before the queue-size read
+// that follows it, so the two round trips overlap.  Entries at or past the
+// queue size are stale and are never used; the queues hold n entries.
+__device__ __forceinline__ uint32_t prefetch_entry(const uint32_t* in, uint32_t n)
+{
+    const uint32_t i = queue_index(0, 0u);
+    uint32_t v = 0;
+    if (i < n) asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(v) : "l"(in + i) : "memory");
+    return v;
+}
+
 // One top-down BFS level L over cnt frontier nodes: each frontier node u
 // (height L) labels every unvisited neighbor v with a residual arc v->u as
 // L+1 (.cu:103-139) and appends it to the next frontier, and to the active
-// queue when it holds excess.
+// queue when it holds excess.  `first` is the thread's first entry (prefetch_entry).
 __device__ __forceinline__ void bfs_level_body(const SolveView& g, uint32_t L, uint32_t cnt,
-                                               uint32_t* s_fr, uint32_t* s_act, uint32_t* s_m,
-                                               unsigned long long& visits)
+                                               uint32_t first, uint32_t* s_fr, uint32_t* s_act,
+                                               uint32_t* s_m, unsigned long long& visits)
 {
     Ctl* ctl = g.ctl;
     const uint32_t* in = (L & 1) ? g.fr[1] : g.fr[0];
@@ -138,10 +190,10 @@ __device__ __forceinline__ void bfs_level_body(const SolveView& g, uint32_t L, u
     uint32_t* gcnt = &ctl->bfs_cnt[(L + 1) % 3];
     const uint32_t newh = L + 1u;
     const bool eager = cnt <= BFS_EAGER_MAX;
-    for (uint32_t base = blockIdx.x * DTPB; base < cnt; base += gridDim.x * DTPB) {
-        const uint32_t i = base + threadIdx.x;
+    for (uint32_t it = 0; it * (gridDim.x * DTPB) < cnt; ++it) {
+        const uint32_t i = queue_index(it, cnt);
         if (i < cnt) {
-            const uint32_t u = __ldcg(in + i);
+            const uint32_t u = (it == 0 && cnt <= SPREAD_MAX) ? first : __ldcg(in + i);
             const int4 nb4 = __ldg(g.nbr + u);
             const uint32_t rv = __ldg(g.rev + u);
             const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
@@ -201,7 +253,7 @@ __device__ __forceinline__ void bfs_level_body(const SolveView& g, uint32_t L, u
 
 __global__ void __launch_bounds__(DTPB) k_bfs_seed(SolveView g)
 {
-    __shared__ uint32_t s_fr[DTPB], s_act[DTPB];
+    __shared__ uint32_t s_fr[DTPB * SWEEP_UNROLL], s_act[DTPB * SWEEP_UNROLL];
     __shared__ uint32_t s_m[8];
     if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
     __syncthreads();
@@ -214,6 +266,7 @@ __global__ void __launch_bounds__(DTPB) k_bfs_level(SolveView g, uint32_t L)
     __shared__ uint32_t s_m[8];
     __shared__ unsigned long long s_red[DTPB / 32];
     Ctl* ctl = g.ctl;
+    const uint32_t first = prefetch_entry((L & 1) ? g.fr[1] : g.fr[0], g.n);
     const uint32_t cnt = min(ldcg(&ctl->bfs_cnt[L % 3]), g.n);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl->bfs_cnt[(L + 2) % 3] = 0u;
@@ -224,7 +277,7 @@ __global__ void __launch_bounds__(DTPB) k_bfs_level(SolveView g, uint32_t L)
     unsigned long long visits = 0;
     if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
     __syncthreads();
-    bfs_level_body(g, L, cnt, s_fr, s_act, s_m, visits);
+    bfs_level_body(g, L, cnt, first, s_fr, s_act, s_m, visits);
     const unsigned long long vs = warp_block_sum(visits, s_red);
     if (threadIdx.x == 0 && vs) atomicAdd(&ctl->bfs_visits, vs);
 }
@@ -353,9 +406,10 @@ __device__ __forceinline__ uint32_t discharge_node(const SolveView& g, uint32_t 
 
 // One discharge round over cnt active nodes: discharge each, stage the nodes
 // that become (or stay) active, append them to the next active queue.
+// `first` is the thread's first entry (prefetch_entry).
 __device__ __forceinline__ void discharge_body(const SolveView& g, uint32_t round, uint32_t cnt,
-                                               uint32_t* s_buf, uint32_t stage_cap, uint32_t* s_m,
-                                               Work& w)
+                                               uint32_t first, uint32_t* s_buf, uint32_t stage_cap,
+                                               uint32_t* s_m, Work& w)
 {
     Ctl* ctl = g.ctl;
     const uint32_t* in = (round & 1) ? g.act[1] : g.act[0];
@@ -363,10 +417,10 @@ __device__ __forceinline__ void discharge_body(const SolveView& g, uint32_t roun
     uint32_t* gcnt = &ctl->act_cnt[(round + 1) % 3];
     const Stage st{s_buf, &s_m[0], stage_cap, gcnt, out};
     const int hops = cnt <= g.chain_max_active ? g.chain_hops : 1;
-    for (uint32_t base = blockIdx.x * DTPB; base < cnt; base += gridDim.x * DTPB) {
-        const uint32_t i = base + threadIdx.x;
+    for (uint32_t it = 0; it * (gridDim.x * DTPB) < cnt; ++it) {
+        const uint32_t i = queue_index(it, cnt);
         if (i < cnt) {
-            uint32_t v = __ldcg(in + i);
+            uint32_t v = (it == 0 && cnt <= SPREAD_MAX) ? first : __ldcg(in + i);
             if (v < g.n) {
                 for (int hop = 1;; ++hop) {
                     v = discharge_node(g, v, st, hop < hops, w);
@@ -410,6 +464,7 @@ __global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
     __shared__ uint32_t s_m[8];
     __shared__ unsigned long long s_red[DTPB / 32];
     Ctl* ctl = g.ctl;
+    const uint32_t first = prefetch_entry((round & 1) ? g.act[1] : g.act[0], g.n);
     const uint32_t cnt = min(ldcg(&ctl->act_cnt[round % 3]), g.n);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl->act_cnt[(round + 2) % 3] = 0u;
@@ -419,7 +474,7 @@ __global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
     Work w;
     if (threadIdx.x == 0) s_m[0] = 0;
     __syncthreads();
-    discharge_body(g, round, cnt, s_buf, DTPB * 5, s_m, w);
+    discharge_body(g, round, cnt, first, s_buf, DTPB * 5, s_m, w);
     reduce_work(ctl, w, 0ull, s_red);
 }
 
@@ -513,9 +568,19 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
     Work w;
     unsigned long long bfs_visits = 0;
     if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
-    for (uint32_t v = blockIdx.x * DTPB + threadIdx.x; v < g.n; v += gridDim.x * DTPB) {
-        const int32_t t = ldcg(g.term + v);
-        g.excess[v] = t > 0 ? (long long)t : 0ll;   // source arc saturated (.cu:69-83)
+    constexpr uint32_t CH = DTPB * SWEEP_UNROLL;
+    for (uint32_t base = blockIdx.x * CH; base < g.n; base += gridDim.x * CH) {
+        int32_t t[SWEEP_UNROLL];
+#pragma unroll
+        for (int j = 0; j < SWEEP_UNROLL; ++j) {
+            const uint32_t v = base + j * DTPB + threadIdx.x;
+            t[j] = v < g.n ? ldcg(g.term + v) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < SWEEP_UNROLL; ++j) {
+            const uint32_t v = base + j * DTPB + threadIdx.x;
+            if (v < g.n) g.excess[v] = t[j] > 0 ? (long long)t[j] : 0ll;   // source arc saturated (.cu:69-83)
+        }
     }
     if (grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok)) {
         unsigned long long rounds_total = 0;
@@ -527,10 +592,11 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
             uint32_t L = 1;
             for (;;) {
+                const uint32_t first = prefetch_entry((L & 1) ? g.fr[1] : g.fr[0], g.n);
                 const uint32_t cnt = min(vload(&ctl->bfs_cnt[L % 3]), g.n);
                 if (cnt == 0) break;
                 if (lead) ctl->bfs_cnt[(L + 2) % 3] = 0u;
-                bfs_level_body(g, L, cnt, s_buf, s_buf + DTPB * 4, s_m, bfs_visits);
+                bfs_level_body(g, L, cnt, first, s_buf, s_buf + DTPB * 4, s_m, bfs_visits);
                 if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
                 ++L;
                 ++levels_total;
@@ -547,6 +613,7 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
             uint32_t r = 0;
             unsigned long long visits = 0;
             for (;;) {
+                const uint32_t first = prefetch_entry((r & 1) ? g.act[1] : g.act[0], g.n);
                 const uint32_t cnt = min(vload(&ctl->act_cnt[r % 3]), g.n);
                 if (cnt == 0) break;
                 if (rounds_total >= p.max_rounds) {
@@ -555,7 +622,7 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
                     break;
                 }
                 if (lead) ctl->act_cnt[(r + 2) % 3] = 0u;
-                discharge_body(g, r, cnt, s_buf, DTPB * 8, s_m, w);
+                discharge_body(g, r, cnt, first, s_buf, DTPB * 8, s_m, w);
                 if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
                 ++r;
                 ++rounds_total;
