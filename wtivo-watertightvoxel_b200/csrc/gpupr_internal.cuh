@@ -60,6 +60,8 @@ struct SolveView {
     int chain_hops;                     // nodes one thread may discharge in a row in
                                         // one round (<= 1: no chaining) ...
     uint32_t chain_max_active;          // ... in rounds of at most this many nodes
+    int bfs_hops;                       // nodes one thread may label in a row in one
+                                        // short BFS step (<= 1: level by level)
 };
 
 // ---------------------------------------------------------------------------

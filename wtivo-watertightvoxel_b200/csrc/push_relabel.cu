@@ -143,6 +143,9 @@ __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr
     }
 }
 
+// Nodes one thread may label in a row in a short BFS step (bfs_step_body).
+constexpr int BFS_CHAIN_HOPS = 4;
+
 // Queues up to this size are spread over every SM (queue_index).
 constexpr uint32_t SPREAD_MAX = 65536u;
 
@@ -313,6 +316,116 @@ __device__ __forceinline__ void stage_push(const SolveView& g, const Stage& st, 
     const uint32_t pos = atomicAdd(st.gcnt, 1u);
     if (pos < g.n) st.out[pos] = u;
     else raise_error(g.ctl, (int)GPUPR_ERR_INVARIANT);
+}
+
+// One BFS step of the persistent engine, label-correcting: a frontier node u
+// with label h(u) gives every neighbor v with a residual arc v->u and a label
+// above h(u)+1 (UNVIS included) the label h(u)+1 by atomicMin.  The first
+// label a node gets queues it (and appends it to the active queue when it
+// holds excess); with `propagate`, a later, lower label queues it again, so
+// that its neighbors are relabelled from it.  With hops > 1 (short frontiers)
+// the thread goes on from one node it labelled, up to `hops` nodes in a row,
+// so one step, one grid barrier, covers several levels of a thin frontier; a
+// node reached first by a longer path is lowered when a shorter one reaches
+// it.  While every improvement propagates the labels converge to BFS
+// distances (every label a node ends with was expanded), and reachability,
+// which decides the end of the solve and the partition, is exact in any
+// case: every labelled node is expanded at least once.  A step processes at
+// most hops * cnt nodes and each queues at most 4, so the caller enables
+// `propagate` only while 4 * hops * cnt <= n (the queues hold n); without it
+// only first labels queue a node, at most once.  Until a chained step has run
+// in this BFS every frontier node is labelled L (`exact`), and u's label is
+// not read.
+__device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, uint32_t cnt,
+                                              uint32_t first, uint32_t* s_fr, uint32_t* s_act,
+                                              uint32_t stage_cap, uint32_t* s_m,
+                                              unsigned long long& visits, int hops, bool propagate,
+                                              bool exact)
+{
+    Ctl* ctl = g.ctl;
+    const uint32_t* in = (L & 1) ? g.fr[1] : g.fr[0];
+    uint32_t* out = (L & 1) ? g.fr[0] : g.fr[1];
+    uint32_t* gcnt = &ctl->bfs_cnt[(L + 1) % 3];
+    const Stage sf{s_fr, &s_m[0], stage_cap, gcnt, out};
+    const Stage sa{s_act, &s_m[1], stage_cap, &ctl->act_cnt[0], g.act[0]};
+    const bool eager = cnt <= BFS_EAGER_MAX;
+    for (uint32_t it = 0; it * (gridDim.x * DTPB) < cnt; ++it) {
+        const uint32_t i = queue_index(it, cnt);
+        if (i < cnt) {
+            uint32_t u = (it == 0 && cnt <= SPREAD_MAX) ? first : __ldcg(in + i);
+            uint32_t hu = exact ? L : ldcg(g.height + u);
+            for (int hop = 1; hu < g.n; ++hop) {   // a queued node is labelled (< n)
+                const int4 nb4 = __ldg(g.nbr + u);
+                const uint32_t rv = __ldg(g.rev + u);
+                const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+                const uint32_t cand = hu + 1u;
+                uint32_t next = UNVIS;
+                ++visits;
+                if (eager) {
+                    // short frontier (latency bound): the neighbors' labels,
+                    // reverse residuals and excesses are loaded at once
+                    uint32_t hv[4], rr[4];
+                    long long xv[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int v = nb[k] < 0 ? 0 : nb[k];
+                        const uint32_t rk = (rv >> (2 * k)) & 3u;
+                        hv[k] = ldcg(g.height + v);
+                        rr[k] = ldcg(g.res + (size_t)v * 4u + rk);
+                        xv[k] = ldcg(g.excess + v);
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int v = nb[k];
+                        if (v < 0 || rr[k] == 0u || hv[k] <= cand) continue;
+                        const uint32_t old = atomicMin(g.height + v, cand);
+                        if (old <= cand) continue;
+                        if (old == UNVIS) {
+                            if (cand < g.n && xv[k] > 0) stage_push(g, sa, (uint32_t)v);
+                        } else if (!propagate) {
+                            continue;
+                        }
+                        if (hop < hops && next == UNVIS) next = (uint32_t)v;
+                        else stage_push(g, sf, (uint32_t)v);
+                    }
+                } else {
+                    // long frontier (traffic bound): most neighbors are already
+                    // labelled, so a residual or excess is read only when needed
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int v = nb[k];
+                        if (v < 0) continue;
+                        if (ldcg(g.height + v) <= cand) continue;
+                        const uint32_t rk = (rv >> (2 * k)) & 3u;
+                        if (ldcg(g.res + (size_t)v * 4u + rk) == 0u) continue;
+                        const uint32_t old = atomicMin(g.height + v, cand);
+                        if (old <= cand) continue;
+                        if (old == UNVIS) {
+                            if (cand < g.n && ldcg(g.excess + v) > 0) stage_push(g, sa, (uint32_t)v);
+                        } else if (!propagate) {
+                            continue;
+                        }
+                        if (hop < hops && next == UNVIS) next = (uint32_t)v;
+                        else stage_push(g, sf, (uint32_t)v);
+                    }
+                }
+                if (next == UNVIS) break;
+                u = next;
+                hu = cand;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_m[2] = min(s_m[0], stage_cap); s_m[3] = min(s_m[1], stage_cap);
+            s_m[0] = 0; s_m[1] = 0;
+            s_m[4] = s_m[2] ? atomicAdd(gcnt, s_m[2]) : 0u;
+            s_m[5] = s_m[3] ? atomicAdd(&ctl->act_cnt[0], s_m[3]) : 0u;
+        }
+        __syncthreads();
+        flush_stage(s_fr, s_m[2], s_m[4], out, g.n, ctl);
+        flush_stage(s_act, s_m[3], s_m[5], g.act[0], g.n, ctl);
+        __syncthreads();
+    }
 }
 
 // Returns the node to discharge next in the same round (chaining: a node
@@ -591,12 +704,21 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
             bfs_seed_body(g, s_buf, s_buf + DTPB * 4, s_m);
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
             uint32_t L = 1;
+            bool exact = true;   // no chained step yet: every frontier node is labelled L
             for (;;) {
                 const uint32_t first = prefetch_entry((L & 1) ? g.fr[1] : g.fr[0], g.n);
                 const uint32_t cnt = min(vload(&ctl->bfs_cnt[L % 3]), g.n);
                 if (cnt == 0) break;
                 if (lead) ctl->bfs_cnt[(L + 2) % 3] = 0u;
-                bfs_level_body(g, L, cnt, first, s_buf, s_buf + DTPB * 4, s_m, bfs_visits);
+                // the same decision in every block: it depends on cnt alone
+                const unsigned long long nn = g.n;
+                const int hops = (g.bfs_hops > 1 && cnt <= SPREAD_MAX &&
+                                  4ull * (unsigned long long)g.bfs_hops * cnt <= nn)
+                                     ? g.bfs_hops : 1;
+                const bool propagate = 4ull * (unsigned long long)hops * cnt <= nn;
+                bfs_step_body(g, L, cnt, first, s_buf, s_buf + DTPB * 4, DTPB * 4, s_m, bfs_visits,
+                              hops, propagate, exact);
+                if (hops > 1) exact = false;
                 if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
                 ++L;
                 ++levels_total;
@@ -815,6 +937,7 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     // slow any graph down (a 2.9M-node torus: 6.6 ms, 10.0 with 32768).  The
     // autotuner may pick another setting.
     gv.chain_hops = opt.chain_hops > 0 ? opt.chain_hops : tuned ? te.chain_hops : 4;
+    gv.bfs_hops = BFS_CHAIN_HOPS;
     gv.chain_max_active = opt.chain_max_active > 0 ? (uint32_t)opt.chain_max_active
                           : tuned                  ? (uint32_t)te.chain_max_active
                           : g.n < 1500000u         ? 131072u
