@@ -211,6 +211,20 @@ def quiet_stdout():
         os.close(dn)
 
 
+def host_cpu():
+    """The host's CPU model and logical CPU count, reported beside CPU timings."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count() or 1}
+
+
 def cpu_baseline(args, seed):
     """Single-threaded BK oracle on a smaller graph of the same family."""
     from oracle import oracle as orc
@@ -221,7 +235,7 @@ def cpu_baseline(args, seed):
     dt = time.perf_counter() - t0
     return {"value": g.n_tets / dt, "unit": "tets/s", "cores": 1, "kind": "port",
             "sample": f"same generator at {g.n_tets} tets (one full cut: reduction + BK + "
-                      f"scatter, {dt:.2f} s, oracle/wtivo_oracle.c)"}
+                      f"scatter, {dt:.2f} s, oracle/wtivo_oracle.c)", "host": host_cpu()}
 
 
 def run_ours(args, world, rank, local):
@@ -794,7 +808,8 @@ def run_reference(args, world, rank, local):
         "cpu_baseline": {"value": round(v, 1), "unit": "tets/s", "cores": threads,
                          "kind": "reference",
                          "sample": "full workload: reference graph_cut_fast (host build on all "
-                                   "host threads + its CUDA solver on this GPU), oracle/_ref"},
+                                   "host threads + its CUDA solver on this GPU), oracle/_ref",
+                         "host": host_cpu()},
         "e2e": {"value": round(v, 1), "unit": "tets/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "clocks": clk.summary(),
