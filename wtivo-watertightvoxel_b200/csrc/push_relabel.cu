@@ -102,7 +102,10 @@ constexpr int SWEEP_UNROLL = 4;
 // Level 1 of the backward BFS: nodes with a residual arc to the sink.  Every
 // other height is reset to UNVIS (.cu:374-379).  s_m[0..5] are the block's
 // staging counters (frontier count, active count, and their flush copies);
-// s_fr and s_act hold DTPB * SWEEP_UNROLL entries each.
+// s_fr and s_act hold DTPB * SWEEP_UNROLL entries each.  With kActive the
+// seeds that hold excess are appended to the active queue (engine 1; the
+// persistent engine finds the active nodes after the BFS, active_sweep_body).
+template <bool kActive>
 __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr, uint32_t* s_act,
                                               uint32_t* s_m)
 {
@@ -119,7 +122,7 @@ __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr
 #pragma unroll
         for (int j = 0; j < SWEEP_UNROLL; ++j) {
             const uint32_t v = base + j * DTPB + threadIdx.x;
-            x[j] = (v < g.n && t[j] < 0) ? ldcg(g.excess + v) : 0ll;
+            x[j] = (kActive && v < g.n && t[j] < 0) ? ldcg(g.excess + v) : 0ll;
             if (v < g.n) g.height[v] = (t[j] < 0) ? 1u : UNVIS;
         }
 #pragma unroll
@@ -127,7 +130,7 @@ __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr
             const uint32_t v = base + j * DTPB + threadIdx.x;
             if (v < g.n && t[j] < 0) {
                 s_fr[atomicAdd(&s_m[0], 1u)] = v;
-                if (1u < g.n && x[j] > 0) s_act[atomicAdd(&s_m[1], 1u)] = v;
+                if (kActive && 1u < g.n && x[j] > 0) s_act[atomicAdd(&s_m[1], 1u)] = v;
             }
         }
         __syncthreads();
@@ -165,6 +168,38 @@ __device__ __forceinline__ uint32_t queue_index(uint32_t it, uint32_t cnt)
         return chunk * 32u + (threadIdx.x & 31u);
     }
     return (it * gridDim.x + blockIdx.x) * DTPB + threadIdx.x;
+}
+
+// The active queue after a BFS of the persistent engine: every node with a
+// label below n and positive excess, appended in node order by one streaming
+// pass (12 bytes a node) instead of a random excess load for each node the
+// BFS labels.  s_act holds DTPB * SWEEP_UNROLL entries; s_m[1], s_m[3] and
+// s_m[5] are its staging counters.
+__device__ __forceinline__ void active_sweep_body(const SolveView& g, uint32_t* s_act, uint32_t* s_m)
+{
+    Ctl* ctl = g.ctl;
+    constexpr uint32_t CH = DTPB * SWEEP_UNROLL;
+    for (uint32_t base = blockIdx.x * CH; base < g.n; base += gridDim.x * CH) {
+        uint32_t h[SWEEP_UNROLL];
+        long long x[SWEEP_UNROLL];
+#pragma unroll
+        for (int j = 0; j < SWEEP_UNROLL; ++j) {
+            const uint32_t v = base + j * DTPB + threadIdx.x;
+            h[j] = v < g.n ? ldcg(g.height + v) : UNVIS;
+            x[j] = v < g.n ? ldcg(g.excess + v) : 0ll;
+        }
+#pragma unroll
+        for (int j = 0; j < SWEEP_UNROLL; ++j)
+            if (h[j] < g.n && x[j] > 0) s_act[atomicAdd(&s_m[1], 1u)] = base + j * DTPB + threadIdx.x;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_m[3] = s_m[1]; s_m[1] = 0;
+            s_m[5] = s_m[3] ? atomicAdd(&ctl->act_cnt[0], s_m[3]) : 0u;
+        }
+        __syncthreads();
+        flush_stage(s_act, s_m[3], s_m[5], g.act[0], g.n, ctl);
+        __syncthreads();
+    }
 }
 
 // A thread's first entry of a short queue (queue_index(0, cnt <= SPREAD_MAX)),
@@ -260,7 +295,7 @@ __global__ void __launch_bounds__(DTPB) k_bfs_seed(SolveView g)
     __shared__ uint32_t s_m[8];
     if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
     __syncthreads();
-    bfs_seed_body(g, s_fr, s_act, s_m);
+    bfs_seed_body<true>(g, s_fr, s_act, s_m);
 }
 
 __global__ void __launch_bounds__(DTPB) k_bfs_level(SolveView g, uint32_t L)
@@ -321,9 +356,9 @@ __device__ __forceinline__ void stage_push(const SolveView& g, const Stage& st, 
 // One BFS step of the persistent engine, label-correcting: a frontier node u
 // with label h(u) gives every neighbor v with a residual arc v->u and a label
 // above h(u)+1 (UNVIS included) the label h(u)+1 by atomicMin.  The first
-// label a node gets queues it (and appends it to the active queue when it
-// holds excess); with `propagate`, a later, lower label queues it again, so
-// that its neighbors are relabelled from it.  With hops > 1 (short frontiers)
+// label a node gets queues it (the active queue is built after the BFS,
+// active_sweep_body); with `propagate`, a later, lower label queues it again,
+// so that its neighbors are relabelled from it.  With hops > 1 (short frontiers)
 // the thread goes on from one node it labelled, up to `hops` nodes in a row,
 // so one step, one grid barrier, covers several levels of a thin frontier; a
 // node reached first by a longer path is lowered when a shorter one reaches
@@ -337,7 +372,7 @@ __device__ __forceinline__ void stage_push(const SolveView& g, const Stage& st, 
 // in this BFS every frontier node is labelled L (`exact`), and u's label is
 // not read.
 __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, uint32_t cnt,
-                                              uint32_t first, uint32_t* s_fr, uint32_t* s_act,
+                                              uint32_t first, uint32_t* s_fr,
                                               uint32_t stage_cap, uint32_t* s_m,
                                               unsigned long long& visits, int hops, bool propagate,
                                               bool exact)
@@ -347,7 +382,6 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
     uint32_t* out = (L & 1) ? g.fr[0] : g.fr[1];
     uint32_t* gcnt = &ctl->bfs_cnt[(L + 1) % 3];
     const Stage sf{s_fr, &s_m[0], stage_cap, gcnt, out};
-    const Stage sa{s_act, &s_m[1], stage_cap, &ctl->act_cnt[0], g.act[0]};
     const bool eager = cnt <= BFS_EAGER_MAX;
     for (uint32_t it = 0; it * (gridDim.x * DTPB) < cnt; ++it) {
         const uint32_t i = queue_index(it, cnt);
@@ -362,35 +396,28 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
                 uint32_t next = UNVIS;
                 ++visits;
                 if (eager) {
-                    // short frontier (latency bound): the neighbors' labels,
-                    // reverse residuals and excesses are loaded at once
+                    // short frontier (latency bound): the neighbors' labels and
+                    // reverse residuals are loaded at once
                     uint32_t hv[4], rr[4];
-                    long long xv[4];
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int v = nb[k] < 0 ? 0 : nb[k];
                         const uint32_t rk = (rv >> (2 * k)) & 3u;
                         hv[k] = ldcg(g.height + v);
                         rr[k] = ldcg(g.res + (size_t)v * 4u + rk);
-                        xv[k] = ldcg(g.excess + v);
                     }
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int v = nb[k];
                         if (v < 0 || rr[k] == 0u || hv[k] <= cand) continue;
                         const uint32_t old = atomicMin(g.height + v, cand);
-                        if (old <= cand) continue;
-                        if (old == UNVIS) {
-                            if (cand < g.n && xv[k] > 0) stage_push(g, sa, (uint32_t)v);
-                        } else if (!propagate) {
-                            continue;
-                        }
+                        if (old <= cand || (old != UNVIS && !propagate)) continue;
                         if (hop < hops && next == UNVIS) next = (uint32_t)v;
                         else stage_push(g, sf, (uint32_t)v);
                     }
                 } else {
                     // long frontier (traffic bound): most neighbors are already
-                    // labelled, so a residual or excess is read only when needed
+                    // labelled, so a residual is read only when needed
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int v = nb[k];
@@ -399,12 +426,7 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
                         const uint32_t rk = (rv >> (2 * k)) & 3u;
                         if (ldcg(g.res + (size_t)v * 4u + rk) == 0u) continue;
                         const uint32_t old = atomicMin(g.height + v, cand);
-                        if (old <= cand) continue;
-                        if (old == UNVIS) {
-                            if (cand < g.n && ldcg(g.excess + v) > 0) stage_push(g, sa, (uint32_t)v);
-                        } else if (!propagate) {
-                            continue;
-                        }
+                        if (old <= cand || (old != UNVIS && !propagate)) continue;
                         if (hop < hops && next == UNVIS) next = (uint32_t)v;
                         else stage_push(g, sf, (uint32_t)v);
                     }
@@ -416,14 +438,12 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            s_m[2] = min(s_m[0], stage_cap); s_m[3] = min(s_m[1], stage_cap);
-            s_m[0] = 0; s_m[1] = 0;
+            s_m[2] = min(s_m[0], stage_cap);
+            s_m[0] = 0;
             s_m[4] = s_m[2] ? atomicAdd(gcnt, s_m[2]) : 0u;
-            s_m[5] = s_m[3] ? atomicAdd(&ctl->act_cnt[0], s_m[3]) : 0u;
         }
         __syncthreads();
         flush_stage(s_fr, s_m[2], s_m[4], out, g.n, ctl);
-        flush_stage(s_act, s_m[3], s_m[5], g.act[0], g.n, ctl);
         __syncthreads();
     }
 }
@@ -701,7 +721,7 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
         bool ok = true;
         while (ok) {
             // ---- exact global relabel ----
-            bfs_seed_body(g, s_buf, s_buf + DTPB * 4, s_m);
+            bfs_seed_body<false>(g, s_buf, s_buf + DTPB * 4, s_m);
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
             uint32_t L = 1;
             bool exact = true;   // no chained step yet: every frontier node is labelled L
@@ -716,8 +736,8 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
                                   4ull * (unsigned long long)g.bfs_hops * cnt <= nn)
                                      ? g.bfs_hops : 1;
                 const bool propagate = 4ull * (unsigned long long)hops * cnt <= nn;
-                bfs_step_body(g, L, cnt, first, s_buf, s_buf + DTPB * 4, DTPB * 4, s_m, bfs_visits,
-                              hops, propagate, exact);
+                bfs_step_body(g, L, cnt, first, s_buf, DTPB * 8, s_m, bfs_visits, hops, propagate,
+                              exact);
                 if (hops > 1) exact = false;
                 if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
                 ++L;
@@ -730,6 +750,8 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
             }
             if (!ok) break;
             ++relabels;
+            active_sweep_body(g, s_buf, s_m);
+            if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
             if (vload(&ctl->act_cnt[0]) == 0u) break;   // maximum preflow
             // ---- discharge rounds ----
             uint32_t r = 0;
