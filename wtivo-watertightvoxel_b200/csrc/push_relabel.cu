@@ -1,5 +1,5 @@
 // push_relabel.cu -- Phase-I multi-discharge push-relabel on the reduced
-// ELL graph, with exact global relabels by backward BFS from the sink.
+// ELL graph, with global relabels by backward BFS from the sink.
 //
 // Replaces cellocut_gpu_push_relabel_fast
 // (native/gpupr/gpu_push_relabel_fast.cu:406-571).  Differences in design:
@@ -12,6 +12,13 @@
 //    once per batch of steps.
 //  * Chained discharge: the thread that takes ownership of a neighbour's
 //    excess may discharge it at once, so excess moves several hops a round.
+//  * Label-correcting BFS steps (persistent engine): labels are lowered by
+//    atomicMin and a thread may label several nodes in a row over a short
+//    frontier, so one grid barrier covers several levels; reachability is
+//    exact in every case and labels converge to distances while lowered
+//    labels propagate.  The active queue is collected after each BFS by a
+//    streaming sweep, in node order (engine 1 appends it during its
+//    level-synchronous BFS, .cu:360-402 and :149-166).
 //  * Reverse slots are precomputed at build time (2 bits per slot), so a push
 //    or a BFS step never searches the neighbor's row (.cu:56-67).
 //  * Queue de-duplication without flags: a node owns its excess; the thread
@@ -21,8 +28,8 @@
 //  * Queue appends are staged in shared memory and written with one global
 //    atomic per block iteration; sink flow and work counters are reduced per
 //    block.
-//  * Exactness by construction: the solve ends only when an exact global
-//    relabel finds no node with excess that can reach the sink, so the
+//  * Exactness by construction: the solve ends only when a global relabel
+//    (reachability exact) finds no node with excess that can reach the sink, so the
 //    returned preflow is maximum and the sink-reachable set is the minimal
 //    sink side of the minimum cut (the reference stops when its queue
 //    empties, .cu:490, then relabels once, .cu:551-556).
