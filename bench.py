@@ -3,7 +3,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = one full graph_cut (reduced-graph build, multi-discharge
-push-relabel with exact global relabels, final residual BFS, label scatter)
+push-relabel with global relabels, final residual BFS, label scatter)
 of the benchmark-scale graph: a seeded defective (3,5) torus-knot tube
 (~2M faces) over a Kuhn lattice of ~80M tets (the stand-in for the
 reference's 12M-point CGAL Delaunay), lambda_fill = 10.

@@ -727,7 +727,7 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
         uint32_t levels_total = 0, relabels = 0;
         bool ok = true;
         while (ok) {
-            // ---- exact global relabel ----
+            // ---- global relabel (label-correcting steps, reachability exact) ----
             bfs_seed_body<false>(g, s_buf, s_buf + DTPB * 4, s_m);
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
             uint32_t L = 1;
