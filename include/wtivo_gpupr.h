@@ -173,6 +173,10 @@ typedef struct {
  * host arrays of n_graphs+1 entries starting at 0.  out_labels is the
  * concatenation of every graph's graph_cut_fast labels; items[g] receives
  * each graph's flows.  One fill_T and one set of options for the batch.
+ * Unless options set chain_hops, chain_max_active or blocks_per_sm, a batch
+ * of at least 16 graphs averaging under 1.5M tets solves with 8 chained
+ * hops in rounds of up to 131072 active nodes on 3 blocks per SM (the
+ * setting that suits small graphs; the union's own size would pick another).
  */
 gpupr_status gpupr_graph_cut_batch(uint32_t n_graphs, const uint64_t* tet_offsets,
                                    const uint64_t* vertex_offsets, const double* vertices,
