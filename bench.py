@@ -18,11 +18,16 @@ reference's 12M-point CGAL Delaunay), lambda_fill = 10.
   cut, CUDA events around it, live in this run) by algorithmic bytes against
   the measured HBM copy bandwidth; its DRAM traffic from an ncu capture; for
   context, the rate at which this GPU serves independent random 4-byte reads.
-* ``batch`` / ``serve`` / ``labels`` / ``audit`` / ``raw`` / ``autotune``: the
-  batched cut of 64 uneven graphs, the serving loop under Poisson arrivals,
-  the tet-centroid label sampler, the watertight audit of the cut surface, a
-  raw integer graph through gpupr_solve_ell, and the autotuner's choice
+* ``batch`` / ``serve`` / ``labels`` / ``audit`` / ``raw`` / ``config1`` /
+  ``noalloc`` / ``autotune``: the batched cut of 64 uneven graphs, the serving
+  loop under Poisson arrivals, the tet-centroid label sampler, the watertight
+  audit (of the cut surface and of a closed 5.24M-face sphere), 16 seeds of
+  the integer raw graph through gpupr_solve_ell (one checked against the BK
+  oracle at full size), the 500k-point proxy Delaunay cut, the
+  allocation-free solve beside the allocating one, and the autotuner's choice
   (tuned on another graph of the same generator).
+* ``solve_only``: the solver's own device time per cut, beside the
+  reference arm's ``solve_seconds`` for the same graph.
 * ``cpu_baseline``: the CPU oracle (single-threaded Boykov-Kolmogorov, with
   the reference's graph reduction) on a bounded sample of the same workload.
 * ``--impl reference``: the reference's own module (compiled from its
@@ -32,6 +37,10 @@ reference's 12M-point CGAL Delaunay), lambda_fill = 10.
 Multi-GPU: a single cut does not shard (every round and BFS level would
 need a boundary exchange), so N GPUs run N independent replicas (weak
 scaling, no collective on the data path); timing is the max over ranks.
+
+``--only LEG[,LEG...]`` runs the timed cut and only the named extra legs
+(e2e, cpu, batch, serve, labels, audit, raw, config1, noalloc, autotune);
+with ``--n-tets`` it makes the small cases that ncu captures use.
 """
 from __future__ import annotations
 
@@ -63,6 +72,9 @@ WORKLOAD = "torus-knot (3,5) tube, 2% patches dropped, inner shell 0.002, noise 
 B_VISIT, B_PUSH, B_BFS = 73, 24, 57
 
 
+LEGS = ("e2e", "cpu", "batch", "serve", "labels", "audit", "raw", "config1", "noalloc", "autotune")
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -82,7 +94,19 @@ def parse():
                     help="time the built-in grid/relabel rule instead of the autotuned table")
     ap.add_argument("--no-audit", action="store_true", help="skip the watertight audit leg")
     ap.add_argument("--no-raw", action="store_true", help="skip the raw integer graph leg (config 4)")
-    return ap.parse_args()
+    ap.add_argument("--raw-seeds", type=int, default=16)
+    ap.add_argument("--no-raw-check", action="store_true",
+                    help="skip the full-size BK check of the first raw seed")
+    ap.add_argument("--only", default="", help="comma list of extra legs to run: " + ",".join(LEGS))
+    a = ap.parse_args()
+    only = {x.strip() for x in a.only.split(",") if x.strip()}
+    bad = only - set(LEGS)
+    if bad:
+        ap.error(f"unknown legs {sorted(bad)}")
+    off = {"e2e": a.no_e2e, "cpu": a.no_cpu_baseline, "batch": a.no_batch, "serve": a.no_serve,
+           "labels": a.no_labels, "audit": a.no_audit, "raw": a.no_raw, "autotune": a.no_autotune}
+    a.legs = (only if only else set(LEGS)) - {k for k, v in off.items() if v}
+    return a
 
 
 def peaks():
@@ -190,6 +214,14 @@ def whole_job(units_per_rank, ms_local, world):
     return ms, world * units_per_rank / (ms * 1e-3)
 
 
+def bench_config(N, free_n, g, args, world):
+    """The workload keys both arms report, so their configs compare equal."""
+    return {"workload": WORKLOAD, "n_tets": int(N), "free_nodes": int(free_n),
+            "lattice": [int(x) for x in g["shape"]], "lambda_fill": 10.0, "seed": args.seed,
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2_flush": "none needed: inputs (2.6 GB topology) exceed the 126 MB L2"}
+
+
 def make_graph(n_tets, seed):
     import synth
 
@@ -246,7 +278,7 @@ def run_ours(args, world, rank, local):
 
     dev = torch.device("cuda", local)
     tune = None
-    if not args.no_autotune:
+    if "autotune" in args.legs:
         # the library's autotuner, run on another graph of the same generator
         # and size (seed + 1); its table then serves the timed cuts
         gt = make_graph(args.n_tets, args.seed + 1)
@@ -325,7 +357,9 @@ def run_ours(args, world, rank, local):
                 "launches_per_step": int(launches / args.steps),
                 "engine": int(stats[-1]["engine"]),
                 "phase_ms_per_step": {"solve": round(sum(s["solve_device_ms"] for s in stats) / args.steps, 3),
-                                      "build": round(sum(s["build_device_ms"] for s in stats) / args.steps, 3)}}
+                                      "build": round(sum(s["build_device_ms"] for s in stats) / args.steps, 3),
+                                      "global_relabel": round(bfs_ms / args.steps, 3),
+                                      "discharge": round(dis_ms / args.steps, 3)}}
     if rank == 0:
         rs = random_sector_rate(dev)
         roofline["random_sector_gbs"] = round(rs, 1)
@@ -336,7 +370,7 @@ def run_ours(args, world, rank, local):
 
     # e2e through the drop-in module: pinned host topology, host V/labels
     e2e = None
-    if not args.no_e2e:
+    if "e2e" in args.legs:
         pt = torch.from_numpy(g["tets"]).pin_memory()
         pn = torch.from_numpy(g["neighbors"]).pin_memory()
         hV = np.ascontiguousarray(g["vertices"])
@@ -412,15 +446,19 @@ def run_ours(args, world, rank, local):
                       "numpy; each step's tets/neighbors copied from pinned memory, step k+1's copy "
                       "on a second stream while step k cuts (serial_ms_per_step: no overlap)"}
         assert np.array_equal(np.asarray(r[0]), out.cpu().numpy()), "e2e labels differ"
+        del bufs, pt, pn, r
 
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, args.seed)
-    batch = run_batch(args, local) if rank == 0 and not args.no_batch else None
-    serve = run_serve(args) if rank == 0 and not args.no_serve else None
-    labels = run_labels(args, local, g) if rank == 0 and not args.no_labels else None
-    audit = run_audit(args, local, g, out, tets, nbrs) if rank == 0 and not args.no_audit else None
-    raw = run_raw(args, local) if rank == 0 and not args.no_raw else None
+    legs = args.legs if rank == 0 else set()
+    cpu = cpu_baseline(args, args.seed) if "cpu" in legs else None
+    batch = run_batch(args, local) if "batch" in legs else None
+    serve = run_serve(args) if "serve" in legs else None
+    labels = run_labels(args, local, g) if "labels" in legs else None
+    audit = run_audit(args, local, g, out, tets, nbrs) if "audit" in legs else None
+    del tets, nbrs, V, L, out
+    torch.cuda.empty_cache()
+    raw = run_raw(args, local) if "raw" in legs else None
+    config1 = run_config1(args, local) if "config1" in legs else None
+    noalloc = run_noalloc(args, local) if "noalloc" in legs else None
 
     s0 = stats[-1]
     line = {
@@ -429,10 +467,10 @@ def run_ours(args, world, rank, local):
         "ms_per_step": round(ms_max, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64 (exact integer flow; FP64 capacities)",
         "data": "synthetic (seeded generator; no CGAL/OpenVDB in the image)",
-        "config": {"workload": WORKLOAD, "n_tets": N, "free_nodes": int(s0["free_n"]),
-                   "lattice": list(g["shape"]), "lambda_fill": 10.0, "seed": args.seed,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2_flush": "none needed: inputs (2.6 GB topology) exceed the 126 MB L2"},
+        "config": bench_config(N, int(s0["free_n"]), g, args, world),
+        "solve_only": {"ms": round(float(np.median([s["solve_device_ms"] for s in stats])), 3),
+                       "what": "median CUDA-event time of the solve phase (push-relabel, every "
+                               "global relabel, final BFS) per cut, inputs in HBM"},
         "flow": int(s0["adjusted_flow"]),
         "solve": {"rounds": int(s0["rounds"]), "global_relabels": int(s0["global_relabels"]),
                   "bfs_levels": int(s0["bfs_levels"]), "node_visits": int(s0["node_visits"]),
@@ -443,7 +481,8 @@ def run_ours(args, world, rank, local):
                   "free_nodes_per_s": round(s0["free_n"] / (s0["solve_device_ms"] * 1e-3), 1),
                   "one_sweep_floor_ms": round(60.0 * s0["free_n"] / (pk["hbm_gbs"] * 1e9) * 1e3, 4)},
         "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
-        "batch": batch, "serve": serve, "labels": labels, "audit": audit, "raw": raw, "autotune": tune,
+        "batch": batch, "serve": serve, "labels": labels, "audit": audit, "raw": raw,
+        "config1": config1, "noalloc": noalloc, "autotune": tune,
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
     }
     return line
@@ -537,12 +576,31 @@ def run_labels(args, local, g):
                              "sample": f"first {n_cpu} tets, oracle/wtivo_oracle.c"}}
 
 
+def _cut_capacity(nbr, cap, src, snk, part):
+    """Capacity of the cut (S = part 0, T = part 1) in the input raw graph."""
+    import torch
+
+    p = part.long()
+    valid = nbr >= 0
+    pu = torch.where(valid, p[nbr.long().clamp_min(0)], torch.zeros_like(nbr).long())
+    nl = (cap.long() * (valid & (p[:, None] == 0) & (pu == 1))).sum()
+    s, k = src.long(), snk.long()
+    return int((nl + torch.where(p == 0, k, torch.zeros_like(k)).sum()
+                + torch.where(p == 1, s, torch.zeros_like(s)).sum()).item())
+
+
 def run_raw(args, local):
-    """Config 4: a raw integer graph (all nodes free, given integer n-links
-    and t-links; gpupr_solve_ell) of 11.7M nodes (125^3-cube Kuhn lattice over
-    uniform space, area-proportional n-links, noisy sphere-SDF t-links),
-    inputs in HBM; checked by the max-flow = min-cut identity; CPU baseline:
-    the BK oracle, 1 core, on the 1.4M-node graph of the same generator."""
+    """Config 4: integer raw graphs (all nodes free, given integer n-links and
+    t-links; gpupr_solve_ell), args.raw_seeds seeds (default 16) of the
+    2M-point size.  Qhull needs about two minutes per 2M-point seed, so the
+    bench uses the lattice stand-in (the Delaunay form is tested at full size
+    in the GPU tests): per seed a 125^3-cube jittered Kuhn lattice of the unit
+    cube (11.7M nodes), n-links round(1e4 area / mean area), noisy sphere-SDF
+    t-links.  Inputs in HBM.  Timed: the seeds one after the other, and all of
+    them as one disjoint-union graph; every seed's flow equals the capacity of
+    its returned cut, the union equals the separate solves, and the first
+    seed's flow and partition are compared with the BK oracle at full size
+    (whose single-core time is the CPU baseline)."""
     import torch
 
     import gpupr_capi
@@ -550,51 +608,170 @@ def run_raw(args, local):
     from oracle import oracle as orc
 
     dev = torch.device("cuda", local)
-    g = synth.config4(args.seed, n_points=2_000_000, use_delaunay=False)
-    nbr, cap, s, k = (torch.from_numpy(np.ascontiguousarray(x)).to(dev)
-                      for x in (g["nbr"], g["cap"].view(np.int32), g["src"].view(np.int32),
-                                g["snk"].view(np.int32)))
-    n = int(nbr.shape[0])
-    stream = torch.cuda.current_stream(dev)
-    for _ in range(3):
-        flow, part, st = gpupr_capi.solve_ell(nbr, cap, s, k)
-    ms = cuda_ms(lambda: gpupr_capi.solve_ell(nbr, cap, s, k), 5, stream)
-    # certificate: capacity of the returned cut in the input graph
-    p = part.long()
-    valid = nbr >= 0
-    pu = torch.where(valid, p[nbr.long().clamp_min(0)], torch.zeros_like(nbr).long())
-    nl = (cap.long() * (valid & (p[:, None] == 0) & (pu == 1))).sum()
-    src, snk = s.long(), k.long()
-    cut = int((nl + torch.where(p == 0, snk, torch.zeros_like(snk)).sum()
-               + torch.where(p == 1, src, torch.zeros_like(src)).sum()).item())
-    gs = synth.config4(args.seed, n_points=250_000, use_delaunay=False)
-    term = (gs["src"].astype(np.int64) - gs["snk"].astype(np.int64)).astype(np.int32)
     t0 = time.perf_counter()
-    orc.maxflow_bk(gs["nbr"], gs["cap"], term)
-    cpu_s = time.perf_counter() - t0
-    return {"config": "raw integer graph, 125^3-cube Kuhn lattice (11.7M nodes), integer n-links "
-                      "round(1e4 area/mean), sphere-SDF t-links, inputs in HBM",
-            "nodes": n, "flow": int(flow), "cut_capacity_equals_flow": bool(cut == flow),
-            "ms": round(ms, 3), "nodes_per_s": round(n / (ms * 1e-3), 1),
-            "solve_device_ms": round(st["solve_device_ms"], 3), "rounds": int(st["rounds"]),
-            "global_relabels": int(st["global_relabels"]),
-            "cpu_baseline": {"value": round(len(gs["nbr"]) / cpu_s, 1), "unit": "nodes/s", "cores": 1,
-                             "kind": "port", "sample": f"{len(gs['nbr'])}-node graph of the same "
-                                                       "generator, BK max flow, oracle/wtivo_oracle.c"}}
+    graphs = [synth.config4(args.seed + k, n_points=2_000_000, use_delaunay=False)
+              for k in range(args.raw_seeds)]
+    gen_s = time.perf_counter() - t0
+    dg = [tuple(torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+                for x in (g["nbr"], g["cap"].view(np.int32), g["src"].view(np.int32),
+                          g["snk"].view(np.int32))) for g in graphs]
+    sizes = [int(d[0].shape[0]) for d in dg]
+    total = int(sum(sizes))
+    stream = torch.cuda.current_stream(dev)
+    for d in dg[:3]:
+        gpupr_capi.solve_ell(*d)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    res = [gpupr_capi.solve_ell(*d) for d in dg]
+    b.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = a.elapsed_time(b)
+    certified = all(_cut_capacity(*d, r[1]) == r[0] for d, r in zip(dg, res))
+    # the seeds as one disjoint-union graph
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    un = (torch.cat([torch.where(d[0] >= 0, d[0] + int(o), d[0]) for d, o in zip(dg, off[:-1])]),
+          *(torch.cat([d[i] for d in dg]) for i in (1, 2, 3)))
+    gpupr_capi.solve_ell(*un)
+    torch.cuda.synchronize()
+    a.record(stream)
+    uflow, upart, ust = gpupr_capi.solve_ell(*un)
+    b.record(stream)
+    torch.cuda.synchronize()
+    union_ms = a.elapsed_time(b)
+    union_same = uflow == sum(r[0] for r in res) and all(
+        torch.equal(upart[int(off[i]):int(off[i + 1])], res[i][1]) for i in range(len(dg)))
+    check = None
+    if not args.no_raw_check:
+        g = graphs[0]
+        src, snk = g["src"].astype(np.int64), g["snk"].astype(np.int64)
+        term = (src - snk).astype(np.int32)
+        t0 = time.perf_counter()
+        f_bk, _, _, p_bk = orc.maxflow_bk(g["nbr"], g["cap"], term)
+        cpu_s = time.perf_counter() - t0
+        check = {"seed": args.seed, "identical_to_oracle": bool(
+                     f_bk + int(np.minimum(src, snk).sum()) == res[0][0]
+                     and np.array_equal(res[0][1].cpu().numpy(), p_bk)),
+                 "oracle_s": round(cpu_s, 2)}
+        cpu = {"value": round(sizes[0] / cpu_s, 1), "unit": "nodes/s", "cores": 1, "kind": "port",
+               "sample": f"seed {args.seed}, {sizes[0]} nodes: BK max flow + partition, "
+                         "oracle/wtivo_oracle.c", "host": host_cpu()}
+    else:
+        cpu = None
+    st0 = res[0][2]
+    return {"config": f"{len(dg)} seeds of the raw integer graph, each a 125^3-cube Kuhn lattice "
+                      "(11.7M nodes; lattice stand-in for the 2M-point Delaunay), integer n-links "
+                      "round(1e4 area/mean), noisy sphere-SDF t-links, inputs in HBM",
+            "seeds": len(dg), "nodes_per_seed": sizes[0], "nodes": total,
+            "flows": [int(r[0]) for r in res], "every_cut_capacity_equals_flow": bool(certified),
+            "sequential_ms": round(seq_ms, 3), "nodes_per_s": round(total / (seq_ms * 1e-3), 1),
+            "union_ms": round(union_ms, 3), "union_nodes_per_s": round(total / (union_ms * 1e-3), 1),
+            "union_identical_to_separate": bool(union_same),
+            "seed0": {"ms": round(st0["solve_device_ms"], 3), "rounds": int(st0["rounds"]),
+                      "global_relabels": int(st0["global_relabels"])},
+            "oracle_check": check, "generation_s_host": round(gen_s, 1), "cpu_baseline": cpu}
 
 
-def run_audit(args, local, g, labels_dev, tets, nbrs):
-    """Edge-degree watertight audit of the benchmark cut's surface (device
-    faces); CPU baseline: the oracle's sort-and-count, 1 core."""
+def run_config1(args, local):
+    """Config 1 at its stated size: holed icosphere (r 0.4, subdivision 5, 5%
+    of faces deleted), 500k-point proxy at res 256, Qhull Delaunay in Morton
+    cell order (~3.2M tets), lambda_fill 10.  Device time of the cut through
+    the C ABI with inputs in HBM, and the drop-in graph_cut_fast with host
+    vertices and labels; labels and flow compared with the oracle, whose
+    single-core time is the CPU baseline."""
     import torch
 
     import gpupr_capi
+    import synth
     import wtivo_gpupr
     from oracle import oracle as orc
 
     dev = torch.device("cuda", local)
-    Vs, F = wtivo_gpupr.surface_extraction_topology_cuda(labels_dev.cpu().numpy(), g["vertices"], tets, nbrs)
-    dF = torch.from_numpy(np.ascontiguousarray(F)).to(dev)
+    g = synth.config1(args.seed, n_points=500_000)
+    tets, nbrs, V, L = (torch.from_numpy(np.ascontiguousarray(g[k])).to(dev)
+                        for k in ("tets", "neighbors", "vertices", "labels"))
+    out = torch.empty(g.n_tets, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        _, st = gpupr_capi.graph_cut(V, tets, nbrs, L, 10.0, out=out)
+    ms = cuda_ms(lambda: gpupr_capi.graph_cut(V, tets, nbrs, L, 10.0, out=out), 5, stream)
+    walls = []
+    for _ in range(5):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = wtivo_gpupr.graph_cut_fast(g["vertices"], tets, nbrs, g["labels"], 10.0)
+        walls.append(time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    lab, ost = orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0)
+    cpu_s = time.perf_counter() - t0
+    same = (np.array_equal(out.cpu().numpy(), lab) and np.array_equal(np.asarray(r[0]), lab)
+            and st["adjusted_flow"] == ost["adjusted_flow"] == int(r[1]))
+    return {"config": "holed icosphere, 500k-point proxy at res 256, Qhull Delaunay (Morton cell "
+                      "order), lambda_fill=10",
+            "n_tets": g.n_tets, "free_nodes": int(st["free_n"]), "flow": int(st["adjusted_flow"]),
+            "ms": round(ms, 3), "tets_per_s": round(g.n_tets / (ms * 1e-3), 1),
+            "solve_device_ms": round(st["solve_device_ms"], 3),
+            "dropin_host_arrays_ms": round(1e3 * float(np.median(walls)), 3),
+            "identical_to_oracle": bool(same),
+            "cpu_baseline": {"value": round(g.n_tets / cpu_s, 1), "unit": "tets/s", "cores": 1,
+                             "kind": "port", "sample": "the whole graph: reduction + BK + scatter, "
+                                                       "oracle/wtivo_oracle.c"}}
+
+
+def run_noalloc(args, local):
+    """The allocation-free solve beside the allocating one on the same reduced
+    graph (a holed-torus lattice of 1M tets, under the 1,048,576-node limit of
+    the static scratch array): median wall time of 5 alternating calls each,
+    the graph's residuals restored before every call; results compared."""
+    import torch
+
+    import gpupr_capi
+    import synth
+
+    dev = torch.device("cuda", local)
+    g = synth.config3_graph(1, 1_000_000, args.seed)
+    tets, nbrs = (torch.from_numpy(np.ascontiguousarray(g[k])).to(dev) for k in ("tets", "neighbors"))
+    b = gpupr_capi.build_reduced(g["vertices"], tets, nbrs, g["labels"], 10.0)
+    n = len(b["nbr"])
+    if n > 1 << 20:
+        return {"skipped": f"{n} free nodes exceed the static scratch limit"}
+    scratch = gpupr_capi.noalloc_prepare()
+    nbr = torch.from_numpy(np.ascontiguousarray(b["nbr"])).to(dev)
+    res0 = torch.from_numpy(np.ascontiguousarray(b["res"]).view(np.int32)).to(dev)
+    term0 = torch.from_numpy(np.ascontiguousarray(b["term"])).to(dev)
+    res, term = res0.clone(), term0.clone()
+    part = torch.empty(n, dtype=torch.uint8, device=dev)
+    t_alloc, t_na = [], []
+    for rep in range(6):
+        for which in (0, 1):
+            res.copy_(res0)
+            term.copy_(term0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if which == 0:
+                pa, sa, _ = gpupr_capi.solve_reduced(nbr, res, term)
+            else:
+                sn = gpupr_capi.solve_reduced_noalloc(nbr, res, term, part)
+            torch.cuda.synchronize()
+            if rep:
+                (t_alloc if which == 0 else t_na).append(time.perf_counter() - t0)
+    same = sa["raw_flow"] == sn["raw_flow"] and np.array_equal(part.cpu().numpy(), pa)
+    return {"config": "holed-torus Kuhn lattice, 1M tets, reduced graph in HBM",
+            "free_nodes": n, "scratch_bytes": scratch,
+            "solve_reduced_ms": round(1e3 * float(np.median(t_alloc)), 3),
+            "solve_reduced_engine": int(sa["engine"]),
+            "noalloc_ms": round(1e3 * float(np.median(t_na)), 3), "noalloc_engine": 1,
+            "identical": bool(same)}
+
+
+def _audit_case(dF, F, dev):
+    """Device time of gpupr_edge_audit on device faces, its roofline, and the
+    oracle's sort-and-count (1 core) on the same faces."""
+    import torch
+
+    import gpupr_capi
+    from oracle import oracle as orc
+
     stream = torch.cuda.current_stream(dev)
     for _ in range(3):
         bad, nbytes = gpupr_capi.edge_audit(dF)
@@ -603,18 +780,41 @@ def run_audit(args, local, g, labels_dev, tets, nbrs):
     ref = orc.edge_audit(F)
     cpu_s = time.perf_counter() - t0
     nf = len(F)
-    cap = nbytes // 12
-    alg = nf * 12 + 3 * nf * 12 + cap * 12 * 2      # faces, 3 edge updates, table clear + scan
+    slots = nbytes // 8
+    # faces 12 B; each of the 3 edge updates reads and writes its 8-byte slot;
+    # the table is cleared (8 B a slot) and scanned (8 B a slot)
+    alg = nf * 12 + 3 * nf * 16 + slots * 16
     pk, pk_kind = peaks()
     gbs = alg / (ms * 1e-3) / 1e9
-    return {"config": "cut surface of the benchmark graph, faces in HBM", "faces": int(nf),
-            "bad_edge_groups": int(bad), "identical_to_oracle": bool(bad == ref),
-            "faces_per_s": round(nf / (ms * 1e-3), 1), "ms": round(ms, 3),
-            "roofline": {"bound": "hbm", "kernel": "k_edge_count + k_edge_bad", "achieved": round(gbs, 1),
-                         "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(gbs / pk["hbm_gbs"], 4),
-                         "peak_source": pk_kind, "algorithmic_bytes": int(alg)},
+    return {"faces": int(nf), "bad_edge_groups": int(bad), "identical_to_oracle": bool(bad == ref),
+            "faces_per_s": round(nf / (ms * 1e-3), 1), "ms": round(ms, 3), "table_bytes": int(nbytes),
+            "roofline": {"bound": "hbm", "kernel": "k_edge_count + k_edge_bad (+ table clear)",
+                         "achieved": round(gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": round(gbs / pk["hbm_gbs"], 4), "peak_source": pk_kind,
+                         "algorithmic_bytes": int(alg)},
             "cpu_baseline": {"value": round(nf / cpu_s, 1), "unit": "faces/s", "cores": 1, "kind": "port",
                              "sample": "all faces, oracle/wtivo_oracle.c (qsort of 3F edge keys)"}}
+
+
+def run_audit(args, local, g, labels_dev, tets, nbrs):
+    """Edge-degree watertight audit: of the benchmark cut's surface (device
+    faces; its 631k faces and table fit in L2) and of a closed 5.24M-face
+    icosphere (subdivision 9, table larger than L2); CPU baseline: the
+    oracle's sort-and-count, 1 core."""
+    import torch
+
+    import synth
+    import wtivo_gpupr
+
+    dev = torch.device("cuda", local)
+    Vs, F = wtivo_gpupr.surface_extraction_topology_cuda(labels_dev.cpu().numpy(), g["vertices"], tets, nbrs)
+    out = {"config": "cut surface of the benchmark graph, faces in HBM",
+           **_audit_case(torch.from_numpy(np.ascontiguousarray(F)).to(dev), F, dev)}
+    _, SF = synth.icosphere(9, 0.4)
+    SF = np.ascontiguousarray(SF, np.int32)
+    out["sphere"] = {"config": "closed icosphere, subdivision 9, faces in HBM",
+                     **_audit_case(torch.from_numpy(SF).to(dev), SF, dev)}
+    return out
 
 
 def run_batch(args, local):
@@ -785,23 +985,27 @@ def run_reference(args, world, rank, local):
     for _ in range(args.warmup):
         r = step()
     torch.cuda.synchronize()
-    times = []
+    times, solve_s = [], []
     with Clocks(local) as clk:
         for _ in range(args.steps):
             t0 = time.perf_counter()
             r = step()
             torch.cuda.synchronize()
             times.append(time.perf_counter() - t0)
+            solve_s.append(float(r[16]))
     ms = 1e3 * float(np.mean(times))
     v = N / (ms * 1e-3)
+    free_n = N - int(r[7]) - int(r[8])      # tets neither fixed source nor fixed sink
     return {
         "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "tets/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "int32/int64 (reference: FP64 host capacities, int CUDA push-relabel)",
+        "dtype": "int32/int64 (exact integer flow; FP64 capacities)",
         "data": "synthetic (seeded generator; no CGAL/OpenVDB in the image)",
-        "config": {"workload": WORKLOAD, "n_tets": N, "lattice": list(g["shape"]),
-                   "lambda_fill": 10.0, "seed": args.seed, "parallelism": "single GPU"},
+        "config": bench_config(N, free_n, g, args, world),
+        "solve_only": {"ms": round(1e3 * float(np.median(solve_s)), 3),
+                       "what": "median of the reference's own solve_seconds per cut (its CUDA "
+                               "push-relabel with global relabels and final BFS; host build excluded)"},
         "flow": int(r[1]), "solve": {"rounds": int(r[11]), "global_relabels": int(r[12]),
                                      "build_seconds": float(r[14]), "solve_seconds": float(r[16]),
                                      "native_total_seconds": float(r[17])},

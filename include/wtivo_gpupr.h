@@ -305,9 +305,9 @@ gpupr_status gpupr_surface_fetch(int32_t* faces, double* vertices_out,
  * an application whose own allocator already owns the device heap, or code
  * that must not enter the CUDA allocator mid-pipeline.  Nothing is allocated
  * on the device or the host on success: the solver's scratch (reverse slots,
- * excess, heights, queues, control block; about 25 MiB) is a static device
- * array inside this library, which every GPU that loads the library holds
- * until the process exits.
+ * arc-pair residual sums, excess, heights, queues, control block; about
+ * 41 MiB) is a static device array inside this library, which every GPU that
+ * loads the library's solver module holds until the process exits.
  *   n            at most 1,048,576 nodes; larger graphs are rejected with
  *                GPUPR_ERR_INVALID_ARGUMENT
  *   d_neighbors  int32[4n], d_residual uint32[4n], d_terminal int32[n]: the
@@ -316,10 +316,19 @@ gpupr_status gpupr_surface_fetch(int32_t* faces, double* vertices_out,
  *   d_partition  uint8[n] device output, 1 = the node reaches the sink
  * The first call on a device looks up the array's device address (with that
  * device current) and caches it; make that first call before any stream
- * capture.  All calls share the one array and it keeps the last call's
- * contents (the call clears what must start at zero): calls whose work
- * overlaps on the GPU, from other streams or threads, race and corrupt each
- * other, so serialise them.
+ * capture.  CUDA loads device modules lazily by default, so the array's
+ * memory is committed when the module is first used: call
+ * gpupr_noalloc_prepare() on each device before the caller's allocator
+ * reserves the device heap (after a cudaDeviceReset, call it again: it looks
+ * the address up anew).  Each call waits on the host for its stream (it reads
+ * the solver's control block back between batches of steps) and returns
+ * with the partition written.  It runs the one-launch-per-step engine (a
+ * host check per 24 discharge rounds or 48 BFS levels), not the persistent
+ * engine of gpupr_solve_reduced, so it is slower on the same graph; the
+ * result is the same.  All calls share the one array and it keeps the last
+ * call's contents (the call clears what must start at zero): calls whose
+ * work overlaps on the GPU, from other streams or threads, race and corrupt
+ * each other, so serialise them.
  */
 gpupr_status gpupr_solve_reduced_noalloc(uint32_t n, int32_t* d_neighbors,
                                          uint32_t* d_residual, int32_t* d_terminal,
@@ -327,6 +336,16 @@ gpupr_status gpupr_solve_reduced_noalloc(uint32_t n, int32_t* d_neighbors,
                                          int32_t global_relabel_period,
                                          uint64_t max_rounds, int32_t local_steps,
                                          void* stream, gpupr_cut_stats* stats);
+
+/*
+ * Set-up of gpupr_solve_reduced_noalloc on the current device (no
+ * counterpart in the reference): loads the solver's device module if CUDA has
+ * not loaded it yet, which commits the static scratch array, and looks up the
+ * array's device address anew.  Call it once per device before the caller's
+ * allocator takes the device heap, and again after a cudaDeviceReset.
+ * scratch_bytes (optional) receives the array's size.
+ */
+gpupr_status gpupr_noalloc_prepare(uint64_t* scratch_bytes);
 
 /*
  * Topology upload (replaces wtivo.py:284-309, topology_to_cuda_chunked):

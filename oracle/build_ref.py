@@ -8,8 +8,12 @@ flags (-O3 --std=c++17 for nvcc, scripts/build_gpupr.py:48; strict IEEE
 doubles on the host: no FMA contraction, like MSVC /fp:precise at :68).
 The module name is ``wtivo_gpupr_ref`` so it can sit beside the product's
 ``wtivo_gpupr``.  It is the reference partition source for the parity tests
-and the ``--impl reference`` arm of bench.py on the GPU box, where the
-built .so travels (oracle/_ref is git-ignored, not gpurun-ignored).
+and the ``--impl reference`` arm of bench.py on a machine with a GPU, which
+uses the prebuilt .so (oracle/_ref is kept out of version control; the built
+file is copied along with the working tree, not rebuilt there).
+
+The reference checkout is read from $WTIVO_REFERENCE_SRC when it is set,
+else from DEFAULT_SRC below.
 
     python oracle/build_ref.py [--src /path/to/reference]
 """
@@ -23,7 +27,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-DEFAULT_SRC = Path("/root/reference")
+DEFAULT_SRC = Path(os.environ.get("WTIVO_REFERENCE_SRC", "/root/reference"))
 
 
 def built_module() -> Path | None:

@@ -22,8 +22,8 @@ from oracle import oracle as orc
 pytestmark = pytest.mark.gpu
 
 
-def _graph():
-    g = cached_graph("lattice", 3, 300_000)
+def _graph(kind, seed, size):
+    g = cached_graph(kind, seed, size)
     return orc.build(g["vertices"], g["tets"], g["neighbors"], g["labels"], g["fill_T"])
 
 
@@ -48,28 +48,35 @@ def _noalloc(nbr, res, term, part, **kw):
 
 
 def test_noalloc_matches_allocating_solve_twice(built):
+    """Two calls in a row: a larger graph, then a smaller, different one, so the
+    second call runs over the first call's leftover heights, queues, reverse
+    slots and pair sums in the shared array.  Each result must equal the
+    allocating gpupr_solve_reduced and the BK oracle, and once the array is
+    committed (gpupr_noalloc_prepare) no call changes the device's free memory."""
     import gpupr_capi
 
-    b = _graph()
-    n = len(b["nbr"])
-    assert n <= 1 << 20
-    # the existing, allocating entry point
-    nbr0, res0, term0 = _upload(b)
-    part0, st0, _ = gpupr_capi.solve_reduced(nbr0, res0, term0)
-    for call in range(2):
+    L = gpupr_capi.lib()
+    nbytes = ctypes.c_uint64(0)
+    assert L.gpupr_noalloc_prepare(ctypes.byref(nbytes)) == 0, L.gpupr_last_error()
+    assert 40 << 20 <= nbytes.value <= 48 << 20
+    graphs = [_graph("lattice", 3, 300_000), _graph("box", 5, 120_000)]
+    assert len(graphs[1]["nbr"]) < len(graphs[0]["nbr"])
+    for b in graphs:
+        n = len(b["nbr"])
+        assert n <= 1 << 20
+        # the existing, allocating entry point
+        nbr0, res0, term0 = _upload(b)
+        part0, st0, _ = gpupr_capi.solve_reduced(nbr0, res0, term0)
         nbr, res, term = _upload(b)
         part = torch.full((n,), 7, dtype=torch.uint8, device="cuda")
         torch.cuda.synchronize()
         free_before = torch.cuda.mem_get_info()[0]
         rc, st = _noalloc(nbr, res, term, part)
         torch.cuda.synchronize()
-        assert rc == 0, gpupr_capi.lib().gpupr_last_error()
-        if call == 1:
-            # module already loaded: the call itself took no device memory
-            assert torch.cuda.mem_get_info()[0] == free_before
+        assert rc == 0, L.gpupr_last_error()
+        assert torch.cuda.mem_get_info()[0] == free_before
         assert st.raw_flow == st0["raw_flow"]
         assert np.array_equal(part.cpu().numpy(), part0)
-        # same final residual graph state class: sink side identical, flow identical
         f_bk, _, _, p_bk = orc.maxflow_bk(b["nbr"], b["res"], b["term"])
         assert st.raw_flow == f_bk and np.array_equal(part.cpu().numpy(), p_bk)
 

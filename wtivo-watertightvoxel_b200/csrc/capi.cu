@@ -174,7 +174,7 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
     const SolveOptions opt = resolve_options(options, local_steps, period, max_rounds);
     SolveWorkspace w;
     SolveResult sr;
-    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.term.p, w, opt, s, sr);
+    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr);
     launches += sr.launches;
 
     const auto p0 = std::chrono::steady_clock::now();
@@ -270,7 +270,7 @@ TuneEntry run_autotune(const double* vertices, uint64_t nv, int v_dev, const int
                 o.chain_max_active = c.cmax;
                 SolveOptions opt = resolve_options(&o, local_steps, 1024, 2000000ull);
                 SolveResult sr;
-                solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.term.p, w, opt, s, sr);
+                solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr);
                 c.ms.push_back(sr.solve_device_ms);
                 c.last = sr;
             }
@@ -404,7 +404,7 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     }
     SolveWorkspace w;
     SolveResult sr;
-    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.term.p, w, opt, s, sr);
+    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr);
     launches += sr.launches;
 
     DevBuf<uint8_t> dout;
@@ -630,12 +630,14 @@ gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_r
         select_device_for(d_neighbors, "graph");
         uint64_t launches = 0;
         DevBuf<uint8_t> rev(n, s);
-        compute_reverse_slots(n, reinterpret_cast<const int4*>(d_neighbors), rev.p, s, &launches);
+        DevBuf<uint32_t> pair((size_t)n * 4u, s);
+        compute_reverse_slots(n, reinterpret_cast<const int4*>(d_neighbors), d_residual, rev.p,
+                              pair.p, s, &launches);
         const SolveOptions opt = resolve_options(nullptr, local_steps, global_relabel_period, max_rounds);
         SolveWorkspace w;
         SolveResult sr;
         solve_push_relabel(n, reinterpret_cast<const int4*>(d_neighbors), d_residual, rev.p,
-                           d_terminal, w, opt, s, sr);
+                           pair.p, d_terminal, w, opt, s, sr);
         launches += sr.launches;
         DevBuf<uint8_t> part(n, s);
         partition_from_height(n, w.height.p, part.p, s, &launches);
@@ -692,12 +694,14 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
         DevBuf<uint32_t> res((size_t)n * 4u, s);
         DevBuf<int32_t> term(n, s);
         DevBuf<uint8_t> rev(n, s);
+        DevBuf<uint32_t> pair((size_t)n * 4u, s);
         const int64_t base = prepare_raw_graph(n, d_cap, d_src, d_snk, d_nbr, res.p, term.p, s, &launches);
-        compute_reverse_slots(n, reinterpret_cast<const int4*>(d_nbr), rev.p, s, &launches);
+        compute_reverse_slots(n, reinterpret_cast<const int4*>(d_nbr), res.p, rev.p, pair.p, s, &launches);
         const SolveOptions opt = resolve_options(options, 8, 1024, 2000000ull);
         SolveWorkspace w;
         SolveResult sr;
-        solve_push_relabel(n, reinterpret_cast<const int4*>(d_nbr), res.p, rev.p, term.p, w, opt, s, sr);
+        solve_push_relabel(n, reinterpret_cast<const int4*>(d_nbr), res.p, rev.p, pair.p, term.p, w,
+                           opt, s, sr);
         launches += sr.launches;
         partition_from_height(n, w.height.p, d_partition, s, &launches);
         GPUPR_CUDA(cudaStreamSynchronize(s));
@@ -705,7 +709,7 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
         if (stats) {
             stats->adjusted_flow = base + sr.raw_flow;
             stats->raw_flow = sr.raw_flow;
-            stats->graph_bytes = res.bytes() + term.bytes() + rev.bytes();
+            stats->graph_bytes = res.bytes() + term.bytes() + rev.bytes() + pair.bytes();
             stats->workspace_bytes = sr.workspace_bytes;
             stats->rounds = sr.rounds;
             stats->global_relabels = sr.relabels;
@@ -789,6 +793,14 @@ gpupr_status gpupr_solve_reduced_noalloc(uint32_t n, int32_t* d_neighbors, uint3
             stats->bfs_levels = sr.bfs_levels;
             stats->kernel_launches = sr.launches;
         }
+    });
+}
+
+gpupr_status gpupr_noalloc_prepare(uint64_t* scratch_bytes)
+{
+    return guarded([&] {
+        const uint64_t b = noalloc_prepare();
+        if (scratch_bytes) *scratch_bytes = b;
     });
 }
 

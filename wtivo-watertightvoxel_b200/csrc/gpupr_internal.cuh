@@ -38,7 +38,9 @@ struct Ctl {
                              // (low 40 bits) | BAR_ABORT once an error is raised
     uint32_t relabel_phases; // persistent engine: global relabels run
     uint32_t pad0;
-    unsigned long long reserved[2];
+    // persistent engine, globaltimer ns of block 0 summed per phase: BFS
+    // (seed + steps), active sweeps, discharge rounds
+    unsigned long long bfs_ns, sweep_ns, discharge_ns, pad1;
 };
 
 constexpr unsigned long long BAR_ABORT = 1ull << 62;
@@ -50,6 +52,10 @@ struct SolveView {
     const int4* __restrict__ nbr;       // [n] neighbor row (reduced ids, -1)
     uint32_t* res;                      // [4n] residual capacity per slot
     const uint8_t* __restrict__ rev;    // [n] 2-bit reverse slot per slot
+    const uint4* __restrict__ pair;     // [n] per slot k: res[v][k] + res[u][rev k], the
+                                        // arc pair's residual sum (u = nbr[v][k]); a push
+                                        // moves residual between the two arcs and keeps it,
+                                        // so r(u->v) = pair - res[v][k] between phases
     int32_t* term;                      // [n] src - snk residual
     long long* excess;                  // [n]
     uint32_t* height;                   // [n]
@@ -162,11 +168,15 @@ struct ReducedGraph {
     DevBuf<int4> nbr;
     DevBuf<uint32_t> res;       // 4n
     DevBuf<uint8_t> rev;
+    DevBuf<uint32_t> pair;      // 4n: cap(u->v) + cap(v->u) per slot
     DevBuf<int32_t> term;
     DevBuf<int32_t> full_to_free;  // N
     DevBuf<uint32_t> free_old;     // n
     DevBuf<uint32_t> base_node;    // n, only when BuildInputs::want_base_node
-    uint64_t graph_bytes() const { return nbr.bytes() + res.bytes() + rev.bytes() + term.bytes(); }
+    uint64_t graph_bytes() const
+    {
+        return nbr.bytes() + res.bytes() + rev.bytes() + pair.bytes() + term.bytes();
+    }
 };
 
 // Classify + compact + build; throws gpupr::Error with reference messages.
@@ -189,9 +199,11 @@ void batch_flows(uint32_t G, const unsigned long long* d_free_off, const int32_t
 void scan_tile_counts(uint32_t ntiles, const uint32_t* d_cnt, unsigned long long* d_off,
                       unsigned long long* d_total, cudaStream_t s, uint64_t* launches);
 
-// Reverse-slot table for a reduced graph given in the reference layout.
-void compute_reverse_slots(uint32_t n, const int4* d_nbr, uint8_t* d_rev, cudaStream_t s,
-                           uint64_t* launches);
+// Reverse-slot table and arc-pair residual sums (pair[v][k] = res[v][k] +
+// res[u][rev k]) of a reduced graph given in the reference layout, from its
+// current residuals.
+void compute_reverse_slots(uint32_t n, const int4* d_nbr, const uint32_t* d_res, uint8_t* d_rev,
+                           uint32_t* d_pair, cudaStream_t s, uint64_t* launches);
 
 // label scatter: out[free_old[q]] = height[q] != UNVIS
 void scatter_partition(uint32_t n, const uint32_t* d_free_old, const uint32_t* d_height,
@@ -237,7 +249,7 @@ struct SolveResult {
     uint64_t rounds = 0, relabels = 0, node_visits = 0, pushes = 0, bfs_visits = 0,
              bfs_levels = 0, launches = 0;
     double solve_s = 0.0, final_relabel_s = 0.0, solve_device_ms = 0.0;
-    double discharge_ms = 0.0, bfs_ms = 0.0;
+    double discharge_ms = 0.0, bfs_ms = 0.0, sweep_ms = 0.0;
     uint64_t discharge_launches = 0, bfs_launches = 0;
     uint64_t workspace_bytes = 0;
     int engine = 1;                // 1 one launch per step, 2 persistent
@@ -263,8 +275,8 @@ int size_class(uint32_t n);
 // On return the workspace heights mark the sink-reachable set
 // (height != UNVIS) of the final residual graph.
 void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const uint8_t* d_rev,
-                        int32_t* d_term, SolveWorkspace& w, const SolveOptions& opt,
-                        cudaStream_t s, SolveResult& out);
+                        const uint32_t* d_pair, int32_t* d_term, SolveWorkspace& w,
+                        const SolveOptions& opt, cudaStream_t s, SolveResult& out);
 
 // Cut-surface extraction (surface.cu): count keeps its result per thread
 // for the following fetch.
@@ -303,7 +315,11 @@ constexpr uint32_t NOALLOC_MAX_NODES = 1u << 20;
 void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t* d_term,
                            uint8_t* d_partition, const SolveOptions& opt, cudaStream_t s,
                            SolveResult& out);
-void compute_reverse_slots_noalloc(uint32_t n, const int4* d_nbr, uint8_t* d_rev, int32_t* d_err,
+// Looks up (again) the static scratch array's device address on the current
+// device, loading its module if needed; returns the array's size in bytes.
+uint64_t noalloc_prepare();
+void compute_reverse_slots_noalloc(uint32_t n, const int4* d_nbr, const uint32_t* d_res,
+                                   uint8_t* d_rev, uint32_t* d_pair, int32_t* d_err,
                                    cudaStream_t s);
 
 // Batched graph cut (capi.cu), used by the C ABI and the serving loop.

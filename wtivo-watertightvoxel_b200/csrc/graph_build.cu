@@ -10,10 +10,12 @@
 //   k_tile_scan  exclusive scan of the tile counts  (serial compaction :179-187)
 //   k_assign     reduced id = rank among free tets in tet order
 //   k_build_rows per free tet: 4 capacities (bit-exact FP64, :65-98), ELL row,
-//                reverse-slot codes, t-link sums, base flow (:253-291)
+//                reverse-slot codes, arc-pair capacity sums, t-link sums,
+//                base flow (:253-291)
 //
 // Layout written to HBM (SoA, one 16-byte row per free node):
-//   nbr int4[F], res uint4[F], rev uint8[F] (2 bits per slot), term int32[F].
+//   nbr int4[F], res uint4[F], rev uint8[F] (2 bits per slot),
+//   pair uint4[F] (cap(v->u) + cap(u->v) per slot), term int32[F].
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -183,13 +185,41 @@ __device__ __forceinline__ bool face_capacity(const double (&P)[4][3], uint8_t l
     return true;
 }
 
+// Capacity of face rk of tet j in j's own direction, computed exactly as the
+// thread that builds j's row computes it (same vertex order, same rounding):
+// the face's three vertices go to positions 0,1,2 in the order face slot rk
+// takes them, and face_capacity<0> runs the same operations on them.
+__device__ __forceinline__ uint32_t reverse_capacity(const double* __restrict__ V, uint64_t nv,
+                                                     int4 tj4, int rk, uint8_t lj, uint8_t li,
+                                                     double fill_T)
+{
+    const int tj[4] = {tj4.x, tj4.y, tj4.z, tj4.w};
+    const int ia = (rk == 3) ? 1 : 0;
+    const int ib = (rk <= 1) ? 1 : 2;
+    const int ic = (rk == 0) ? 2 : 3;
+    const int pick[3] = {tj[ia], tj[ib], tj[ic]};
+    double Q[4][3];
+    Q[3][0] = Q[3][1] = Q[3][2] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (pick[k] < 0 || (uint64_t)pick[k] >= nv) return 0u;   // j's own row reports it
+        const double* p = V + (size_t)pick[k] * 3u;
+        Q[k][0] = __ldg(p);
+        Q[k][1] = __ldg(p + 1);
+        Q[k][2] = __ldg(p + 2);
+    }
+    int32_t cap = 0;
+    if (!face_capacity<0>(Q, lj, li, fill_T, &cap)) return 0u;
+    return (uint32_t)cap;
+}
+
 __global__ void __launch_bounds__(TPB) k_build_rows(
     uint32_t F, uint64_t N, const double* __restrict__ V, uint64_t nv,
     const int4* __restrict__ tets, const int4* __restrict__ nbrs,
     const uint8_t* __restrict__ labels, const int32_t* __restrict__ full_to_free,
     const uint32_t* __restrict__ free_old, double fill_T, int4* __restrict__ out_nbr,
-    uint4* __restrict__ out_res, uint8_t* __restrict__ out_rev, int32_t* __restrict__ out_term,
-    uint32_t* __restrict__ out_base, BuildCtl* ctl)
+    uint4* __restrict__ out_res, uint8_t* __restrict__ out_rev, uint4* __restrict__ out_pair,
+    int32_t* __restrict__ out_term, uint32_t* __restrict__ out_base, BuildCtl* ctl)
 {
     __shared__ unsigned long long sh[TPB / 32];
     unsigned long long refs = 0, terms = 0;
@@ -214,13 +244,17 @@ __global__ void __launch_bounds__(TPB) k_build_rows(
         long long src = 0, snk = 0;
         int on[4] = {-1, -1, -1, -1};
         uint32_t orr[4] = {0u, 0u, 0u, 0u};
+        uint32_t opr[4] = {0u, 0u, 0u, 0u};
         uint32_t rv = 0;
         int32_t caps[4];
         int32_t ms[4];
-        ok &= face_capacity<0>(P, li, __ldg(labels + row[0]), fill_T, &caps[0]);
-        ok &= face_capacity<1>(P, li, __ldg(labels + row[1]), fill_T, &caps[1]);
-        ok &= face_capacity<2>(P, li, __ldg(labels + row[2]), fill_T, &caps[2]);
-        ok &= face_capacity<3>(P, li, __ldg(labels + row[3]), fill_T, &caps[3]);
+        uint8_t lj[4];
+#pragma unroll
+        for (int fi = 0; fi < 4; ++fi) lj[fi] = __ldg(labels + row[fi]);
+        ok &= face_capacity<0>(P, li, lj[0], fill_T, &caps[0]);
+        ok &= face_capacity<1>(P, li, lj[1], fill_T, &caps[1]);
+        ok &= face_capacity<2>(P, li, lj[2], fill_T, &caps[2]);
+        ok &= face_capacity<3>(P, li, lj[3], fill_T, &caps[3]);
 #pragma unroll
         for (int fi = 0; fi < 4; ++fi) ms[fi] = __ldg(full_to_free + row[fi]);
 #pragma unroll
@@ -244,6 +278,9 @@ __global__ void __launch_bounds__(TPB) k_build_rows(
                     rk = 0;
                 }
                 rv |= (uint32_t)rk << (2 * fi);
+                // both caps are below 2^30, so the sum fits 32 bits
+                opr[fi] = (uint32_t)cap + reverse_capacity(V, nv, __ldg(tets + j), rk, lj[fi], li,
+                                                           fill_T);
             } else if (m == -2) {
                 src += cap;
                 ++terms;
@@ -263,6 +300,7 @@ __global__ void __launch_bounds__(TPB) k_build_rows(
         out_nbr[q] = make_int4(on[0], on[1], on[2], on[3]);
         out_res[q] = make_uint4(orr[0], orr[1], orr[2], orr[3]);
         out_rev[q] = (uint8_t)rv;
+        out_pair[q] = make_uint4(opr[0], opr[1], opr[2], opr[3]);
         out_term[q] = (int32_t)diff;
     }
     const unsigned long long r = block_sum(refs, sh);
@@ -273,13 +311,21 @@ __global__ void __launch_bounds__(TPB) k_build_rows(
     if (threadIdx.x == 0 && b) atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->base_flow), (unsigned long long)b);
 }
 
+// Reverse slots and arc-pair residual sums of a graph in the reference
+// layout.  A pair sum above 2^32 - 1 (residuals the solver's uint32 arcs
+// cannot hold once pushed) is reported as GPUPR_ERR_BUILD.
 __global__ void __launch_bounds__(TPB) k_reverse_slots(uint32_t n, const int4* __restrict__ nbr,
-                                                       uint8_t* __restrict__ rev, int32_t* err)
+                                                       const uint4* __restrict__ res,
+                                                       uint8_t* __restrict__ rev,
+                                                       uint4* __restrict__ pair, int32_t* err)
 {
     for (uint32_t v = blockIdx.x * TPB + threadIdx.x; v < n; v += gridDim.x * TPB) {
         const int4 r4 = __ldg(nbr + v);
+        const uint4 c4 = __ldg(res + v);
         const int row[4] = {r4.x, r4.y, r4.z, r4.w};
+        const uint32_t own[4] = {c4.x, c4.y, c4.z, c4.w};
         uint32_t rv = 0;
+        uint32_t pr[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int u = row[k];
@@ -293,8 +339,14 @@ __global__ void __launch_bounds__(TPB) k_reverse_slots(uint32_t n, const int4* _
             if (b.x == (int)v) rk = 0;
             if (rk < 0) { atomicExch(err, (int)GPUPR_ERR_NO_REVERSE); rk = 0; }
             rv |= (uint32_t)rk << (2 * k);
+            const unsigned long long sum =
+                (unsigned long long)own[k] +
+                __ldg(reinterpret_cast<const uint32_t*>(res) + (size_t)u * 4u + rk);
+            if (sum > 0xFFFFFFFFull) { atomicExch(err, (int)GPUPR_ERR_BUILD); continue; }
+            pr[k] = (uint32_t)sum;
         }
         rev[v] = (uint8_t)rv;
+        pair[v] = make_uint4(pr[0], pr[1], pr[2], pr[3]);
     }
 }
 
@@ -392,13 +444,14 @@ void build_reduced_graph(const BuildInputs& in, ReducedGraph& g, BuildInfo& info
     g.nbr = DevBuf<int4>(F, s);
     g.res = DevBuf<uint32_t>((size_t)F * 4u, s);
     g.rev = DevBuf<uint8_t>(F, s);
+    g.pair = DevBuf<uint32_t>((size_t)F * 4u, s);
     g.term = DevBuf<int32_t>(F, s);
     if (in.want_base_node) g.base_node = DevBuf<uint32_t>(F, s);
     k_build_rows<<<grid_for(F), TPB, 0, s>>>(
         F, N, in.d_vertices, in.nv, reinterpret_cast<const int4*>(in.d_tets),
         reinterpret_cast<const int4*>(in.d_nbrs), in.d_labels, g.full_to_free.p, g.free_old.p,
-        in.fill_T, g.nbr.p, reinterpret_cast<uint4*>(g.res.p), g.rev.p, g.term.p, g.base_node.p,
-        ctl.p);
+        in.fill_T, g.nbr.p, reinterpret_cast<uint4*>(g.res.p), g.rev.p,
+        reinterpret_cast<uint4*>(g.pair.p), g.term.p, g.base_node.p, ctl.p);
     GPUPR_CUDA(cudaGetLastError());
     *launches += 1;
     GPUPR_CUDA(cudaMemcpyAsync(&h, ctl.p, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -422,21 +475,31 @@ void scan_tile_counts(uint32_t ntiles, const uint32_t* d_cnt, unsigned long long
     *launches += 1;
 }
 
-void compute_reverse_slots(uint32_t n, const int4* d_nbr, uint8_t* d_rev, cudaStream_t s,
-                           uint64_t* launches)
+namespace {
+void raise_reverse_error(int32_t e)
+{
+    if (e == GPUPR_ERR_NO_REVERSE)
+        throw Error{GPUPR_ERR_NO_REVERSE,
+                    "GPUPr-B200 device invariant failed: neighbor lists are not symmetric"};
+    if (e == GPUPR_ERR_BUILD)
+        throw Error{GPUPR_ERR_BUILD, "residual pair sum exceeds the uint32 arc range"};
+    if (e) throw Error{GPUPR_ERR_INVARIANT, "GPUPr-B200 device invariant failed: neighbor id >= n"};
+}
+}  // namespace
+
+void compute_reverse_slots(uint32_t n, const int4* d_nbr, const uint32_t* d_res, uint8_t* d_rev,
+                           uint32_t* d_pair, cudaStream_t s, uint64_t* launches)
 {
     DevBuf<int32_t> err(1, s);
     GPUPR_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int32_t), s));
-    k_reverse_slots<<<grid_for(n), TPB, 0, s>>>(n, d_nbr, d_rev, err.p);
+    k_reverse_slots<<<grid_for(n), TPB, 0, s>>>(n, d_nbr, reinterpret_cast<const uint4*>(d_res),
+                                                d_rev, reinterpret_cast<uint4*>(d_pair), err.p);
     GPUPR_CUDA(cudaGetLastError());
     *launches += 1;
     int32_t e = 0;
     GPUPR_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(e), cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaStreamSynchronize(s));
-    if (e == GPUPR_ERR_NO_REVERSE)
-        throw Error{GPUPR_ERR_NO_REVERSE,
-                    "GPUPr-B200 device invariant failed: neighbor lists are not symmetric"};
-    if (e) throw Error{GPUPR_ERR_INVARIANT, "GPUPr-B200 device invariant failed: neighbor id >= n"};
+    raise_reverse_error(e);
 }
 
 void scatter_partition(uint32_t n, const uint32_t* d_free_old, const uint32_t* d_height,
@@ -463,19 +526,18 @@ namespace gpupr {
 
 // Reverse slots with a caller-provided device error flag (no allocation);
 // used by the allocation-free solve.
-void compute_reverse_slots_noalloc(uint32_t n, const int4* d_nbr, uint8_t* d_rev, int32_t* d_err,
+void compute_reverse_slots_noalloc(uint32_t n, const int4* d_nbr, const uint32_t* d_res,
+                                   uint8_t* d_rev, uint32_t* d_pair, int32_t* d_err,
                                    cudaStream_t s)
 {
     GPUPR_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int32_t), s));
-    k_reverse_slots<<<grid_for(n), TPB, 0, s>>>(n, d_nbr, d_rev, d_err);
+    k_reverse_slots<<<grid_for(n), TPB, 0, s>>>(n, d_nbr, reinterpret_cast<const uint4*>(d_res),
+                                                d_rev, reinterpret_cast<uint4*>(d_pair), d_err);
     GPUPR_CUDA(cudaGetLastError());
     int32_t e = 0;
     GPUPR_CUDA(cudaMemcpyAsync(&e, d_err, sizeof(e), cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaStreamSynchronize(s));
-    if (e == GPUPR_ERR_NO_REVERSE)
-        throw Error{GPUPR_ERR_NO_REVERSE,
-                    "GPUPr-B200 device invariant failed: neighbor lists are not symmetric"};
-    if (e) throw Error{GPUPR_ERR_INVARIANT, "GPUPr-B200 device invariant failed: neighbor id >= n"};
+    raise_reverse_error(e);
 }
 
 }  // namespace gpupr

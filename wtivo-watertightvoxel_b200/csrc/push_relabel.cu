@@ -20,7 +20,12 @@
 //    streaming sweep, in node order (engine 1 appends it during its
 //    level-synchronous BFS, .cu:360-402 and :149-166).
 //  * Reverse slots are precomputed at build time (2 bits per slot), so a push
-//    or a BFS step never searches the neighbor's row (.cu:56-67).
+//    never searches the neighbor's row (.cu:56-67).
+//  * The backward BFS reads no residual of the neighbour it labels: each arc
+//    pair keeps the sum of its two residuals (pushes move residual between
+//    the two arcs and never change the sum), so r(v->u) = pair[u][k] -
+//    res[u][k] comes from the frontier node u's own rows (.cu:103-139 read
+//    the neighbour's row and searched it for the reverse slot).
 //  * Queue de-duplication without flags: a node owns its excess; the thread
 //    whose atomic add moves a node's excess from 0 to positive enqueues it,
 //    and a discharged node that keeps excess re-enqueues itself (.cu:168-178
@@ -98,7 +103,9 @@ __global__ void __launch_bounds__(DTPB) k_init_excess(uint32_t n, const int32_t*
     }
 }
 
-// Frontier size up to which a BFS level loads every neighbor's state at once.
+// Frontier size up to which a BFS level of the one-launch-per-step engine
+// loads the excess of every neighbour with an arc into the frontier node at
+// once (above it, only the excess of a node it labels).
 constexpr uint32_t BFS_EAGER_MAX = 32768u;
 
 // Nodes per thread in the whole-array passes (BFS seed, excess init): that
@@ -221,6 +228,19 @@ __device__ __forceinline__ uint32_t prefetch_entry(const uint32_t* in, uint32_t 
     return v;
 }
 
+// The neighbours v of frontier node u with a residual arc v -> u, from u's
+// own rows: r(v->u) = pair[u][k] - res[u][k] (exact between phases, when no
+// push is in flight).  Returns u's neighbour row; bit k of *arcs is slot k.
+__device__ __forceinline__ int4 residual_in_arcs(const SolveView& g, uint32_t u, uint32_t* arcs)
+{
+    const int4 nb4 = __ldg(g.nbr + u);
+    const uint4 p4 = __ldg(g.pair + u);
+    const uint4 r4 = __ldcg(reinterpret_cast<const uint4*>(g.res) + u);
+    *arcs = (uint32_t)(nb4.x >= 0 && p4.x > r4.x) | ((uint32_t)(nb4.y >= 0 && p4.y > r4.y) << 1) |
+            ((uint32_t)(nb4.z >= 0 && p4.z > r4.z) << 2) | ((uint32_t)(nb4.w >= 0 && p4.w > r4.w) << 3);
+    return nb4;
+}
+
 // One top-down BFS level L over cnt frontier nodes: each frontier node u
 // (height L) labels every unvisited neighbor v with a residual arc v->u as
 // L+1 (.cu:103-139) and appends it to the next frontier, and to the active
@@ -239,28 +259,28 @@ __device__ __forceinline__ void bfs_level_body(const SolveView& g, uint32_t L, u
         const uint32_t i = queue_index(it, cnt);
         if (i < cnt) {
             const uint32_t u = (it == 0 && cnt <= SPREAD_MAX) ? first : __ldcg(in + i);
-            const int4 nb4 = __ldg(g.nbr + u);
-            const uint32_t rv = __ldg(g.rev + u);
+            uint32_t arcs;
+            const int4 nb4 = residual_in_arcs(g, u, &arcs);
             const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+            bool arc[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) arc[k] = (arcs >> k) & 1u;
             ++visits;
             if (eager) {
-                // small frontier (latency bound): the neighbors' heights,
-                // reverse residuals and excesses are loaded at once, one
+                // small frontier (latency bound): the heights and excesses of
+                // the neighbours with an arc into u are loaded at once, one
                 // round trip, then tested
-                uint32_t hv[4], rr[4];
+                uint32_t hv[4];
                 long long xv[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    const int v = nb[k] < 0 ? 0 : nb[k];
-                    const uint32_t rk = (rv >> (2 * k)) & 3u;
-                    hv[k] = ldcg(g.height + v);
-                    rr[k] = ldcg(g.res + (size_t)v * 4u + rk);
-                    xv[k] = ldcg(g.excess + v);
+                    hv[k] = arc[k] ? ldcg(g.height + nb[k]) : 0u;
+                    xv[k] = arc[k] ? ldcg(g.excess + nb[k]) : 0ll;
                 }
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int v = nb[k];
-                    if (v < 0 || hv[k] != UNVIS || rr[k] == 0u) continue;
+                    if (!arc[k] || hv[k] != UNVIS) continue;
                     if (atomicCAS(g.height + v, UNVIS, newh) == UNVIS) {
                         s_fr[atomicAdd(&s_m[0], 1u)] = (uint32_t)v;
                         if (newh < g.n && xv[k] > 0) s_act[atomicAdd(&s_m[1], 1u)] = (uint32_t)v;
@@ -268,14 +288,12 @@ __device__ __forceinline__ void bfs_level_body(const SolveView& g, uint32_t L, u
                 }
             } else {
                 // large frontier (traffic bound): most neighbors are already
-                // labeled, so a residual or excess is read only when needed
+                // labeled, so an excess is read only for a node labelled here
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int v = nb[k];
-                    if (v < 0) continue;
+                    if (!arc[k]) continue;
                     if (ldcg(g.height + v) != UNVIS) continue;
-                    const uint32_t rk = (rv >> (2 * k)) & 3u;
-                    if (ldcg(g.res + (size_t)v * 4u + rk) == 0u) continue;
                     if (atomicCAS(g.height + v, UNVIS, newh) == UNVIS) {
                         s_fr[atomicAdd(&s_m[0], 1u)] = (uint32_t)v;
                         if (newh < g.n && ldcg(g.excess + v) > 0) s_act[atomicAdd(&s_m[1], 1u)] = (uint32_t)v;
@@ -389,54 +407,31 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
     uint32_t* out = (L & 1) ? g.fr[0] : g.fr[1];
     uint32_t* gcnt = &ctl->bfs_cnt[(L + 1) % 3];
     const Stage sf{s_fr, &s_m[0], stage_cap, gcnt, out};
-    const bool eager = cnt <= BFS_EAGER_MAX;
     for (uint32_t it = 0; it * (gridDim.x * DTPB) < cnt; ++it) {
         const uint32_t i = queue_index(it, cnt);
         if (i < cnt) {
             uint32_t u = (it == 0 && cnt <= SPREAD_MAX) ? first : __ldcg(in + i);
             uint32_t hu = exact ? L : ldcg(g.height + u);
             for (int hop = 1; hu < g.n; ++hop) {   // a queued node is labelled (< n)
-                const int4 nb4 = __ldg(g.nbr + u);
-                const uint32_t rv = __ldg(g.rev + u);
+                uint32_t arcs;
+                const int4 nb4 = residual_in_arcs(g, u, &arcs);
                 const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
                 const uint32_t cand = hu + 1u;
                 uint32_t next = UNVIS;
                 ++visits;
-                if (eager) {
-                    // short frontier (latency bound): the neighbors' labels and
-                    // reverse residuals are loaded at once
-                    uint32_t hv[4], rr[4];
+                // the labels of the neighbours with an arc into u, loaded at
+                // once (one round trip), then lowered where above cand
+                uint32_t hv[4];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int v = nb[k] < 0 ? 0 : nb[k];
-                        const uint32_t rk = (rv >> (2 * k)) & 3u;
-                        hv[k] = ldcg(g.height + v);
-                        rr[k] = ldcg(g.res + (size_t)v * 4u + rk);
-                    }
+                for (int k = 0; k < 4; ++k) hv[k] = ((arcs >> k) & 1u) ? ldcg(g.height + nb[k]) : 0u;
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int v = nb[k];
-                        if (v < 0 || rr[k] == 0u || hv[k] <= cand) continue;
-                        const uint32_t old = atomicMin(g.height + v, cand);
-                        if (old <= cand || (old != UNVIS && !propagate)) continue;
-                        if (hop < hops && next == UNVIS) next = (uint32_t)v;
-                        else stage_push(g, sf, (uint32_t)v);
-                    }
-                } else {
-                    // long frontier (traffic bound): most neighbors are already
-                    // labelled, so a residual is read only when needed
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int v = nb[k];
-                        if (v < 0) continue;
-                        if (ldcg(g.height + v) <= cand) continue;
-                        const uint32_t rk = (rv >> (2 * k)) & 3u;
-                        if (ldcg(g.res + (size_t)v * 4u + rk) == 0u) continue;
-                        const uint32_t old = atomicMin(g.height + v, cand);
-                        if (old <= cand || (old != UNVIS && !propagate)) continue;
-                        if (hop < hops && next == UNVIS) next = (uint32_t)v;
-                        else stage_push(g, sf, (uint32_t)v);
-                    }
+                for (int k = 0; k < 4; ++k) {
+                    const int v = nb[k];
+                    if (!((arcs >> k) & 1u) || hv[k] <= cand) continue;
+                    const uint32_t old = atomicMin(g.height + v, cand);
+                    if (old <= cand || (old != UNVIS && !propagate)) continue;
+                    if (hop < hops && next == UNVIS) next = (uint32_t)v;
+                    else stage_push(g, sf, (uint32_t)v);
                 }
                 if (next == UNVIS) break;
                 u = next;
@@ -695,7 +690,7 @@ __device__ bool grid_barrier(Ctl* ctl, unsigned long long& target, unsigned long
     return *s_ok != 0;
 }
 
-__global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistParams p)
+__global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, PersistParams p)
 {
     __shared__ uint32_t s_buf[DTPB * 8];
     __shared__ uint32_t s_m[8];
@@ -707,6 +702,17 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
     unsigned long long bar_target = 0;
     Work w;
     unsigned long long bfs_visits = 0;
+    // phase clock of block 0, read after each phase's closing barrier:
+    // s_clk = {BFS, active sweep, discharge, last mark} (shared memory, so it
+    // holds no registers through the solve)
+    __shared__ unsigned long long s_clk[4];
+    auto lap = [&](int phase) {
+        if (lead) {
+            const unsigned long long t = gtimer();
+            s_clk[phase] += t - s_clk[3];
+            s_clk[3] = t;
+        }
+    };
     if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
     constexpr uint32_t CH = DTPB * SWEEP_UNROLL;
     for (uint32_t base = blockIdx.x * CH; base < g.n; base += gridDim.x * CH) {
@@ -726,6 +732,7 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
         unsigned long long rounds_total = 0;
         uint32_t levels_total = 0, relabels = 0;
         bool ok = true;
+        if (lead) { s_clk[0] = s_clk[1] = s_clk[2] = 0ull; s_clk[3] = gtimer(); }
         while (ok) {
             // ---- global relabel (label-correcting steps, reachability exact) ----
             bfs_seed_body<false>(g, s_buf, s_buf + DTPB * 4, s_m);
@@ -757,8 +764,10 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
             }
             if (!ok) break;
             ++relabels;
+            lap(0);
             active_sweep_body(g, s_buf, s_m);
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
+            lap(1);
             if (vload(&ctl->act_cnt[0]) == 0u) break;   // maximum preflow
             // ---- discharge rounds ----
             uint32_t r = 0;
@@ -786,11 +795,15 @@ __global__ void __launch_bounds__(DTPB) k_solve_persistent(SolveView g, PersistP
                 for (int k = 0; k < 3; ++k) { ctl->act_cnt[k] = 0u; ctl->bfs_cnt[k] = 0u; }
             }
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
+            lap(2);
         }
         if (lead) {
             ctl->rounds_done = (uint32_t)rounds_total;
             ctl->bfs_levels = levels_total;
             ctl->relabel_phases = relabels;
+            ctl->bfs_ns = s_clk[0];
+            ctl->sweep_ns = s_clk[1];
+            ctl->discharge_ns = s_clk[2];
         }
     }
     reduce_work(ctl, w, bfs_visits, s_red);
@@ -1003,12 +1016,16 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     out.bfs_levels = hc.bfs_levels;
     out.solve_device_ms = ms;
     out.discharge_launches = 1;
+    // phase split from block 0's clock; the active sweeps count as relabel work
+    out.bfs_ms = (double)(hc.bfs_ns + hc.sweep_ns) * 1e-6;
+    out.discharge_ms = (double)hc.discharge_ns * 1e-6;
+    out.sweep_ms = (double)hc.sweep_ns * 1e-6;
     out.solve_s = std::chrono::duration<double>(Clock::now() - t0).count();
 }
 
 void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const uint8_t* d_rev,
-                        int32_t* d_term, SolveWorkspace& w, const SolveOptions& opt,
-                        cudaStream_t s, SolveResult& out)
+                        const uint32_t* d_pair, int32_t* d_term, SolveWorkspace& w,
+                        const SolveOptions& opt, cudaStream_t s, SolveResult& out)
 {
     using Clock = std::chrono::steady_clock;
     out = SolveResult{};
@@ -1028,6 +1045,7 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
     g.nbr = d_nbr;
     g.res = d_res;
     g.rev = d_rev;
+    g.pair = reinterpret_cast<const uint4*>(d_pair);
     g.term = d_term;
     g.excess = w.excess.p;
     g.height = w.height.p;
@@ -1197,7 +1215,8 @@ namespace {
 
 constexpr size_t NA_ALIGN = 256;
 constexpr size_t na_round(size_t b) { return (b + NA_ALIGN - 1) / NA_ALIGN * NA_ALIGN; }
-// layout: control block | error flag | excess | height | 3 queues | reverse slots
+// layout: control block | error flag | excess | height | 3 queues | reverse
+// slots | arc-pair residual sums
 constexpr size_t NA_CTL = 0;
 constexpr size_t NA_ERR = na_round(sizeof(Ctl));
 constexpr size_t NA_EXCESS = NA_ERR + NA_ALIGN;
@@ -1206,7 +1225,8 @@ constexpr size_t NA_Q0 = NA_HEIGHT + na_round((size_t)NOALLOC_MAX_NODES * 4u);
 constexpr size_t NA_Q1 = NA_Q0 + na_round((size_t)NOALLOC_MAX_NODES * 4u);
 constexpr size_t NA_Q2 = NA_Q1 + na_round((size_t)NOALLOC_MAX_NODES * 4u);
 constexpr size_t NA_REV = NA_Q2 + na_round((size_t)NOALLOC_MAX_NODES * 4u);
-constexpr size_t NA_BYTES = NA_REV + na_round((size_t)NOALLOC_MAX_NODES);
+constexpr size_t NA_PAIR = NA_REV + na_round((size_t)NOALLOC_MAX_NODES);
+constexpr size_t NA_BYTES = NA_PAIR + na_round((size_t)NOALLOC_MAX_NODES * 16u);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
@@ -1215,19 +1235,26 @@ unsigned char* g_na_ptr[64] = {};
 
 // Device address of the scratch array on the current device.  The host-side
 // name g_noalloc_scratch is only a stand-in for the symbol, so the address is
-// looked up once per device (with that device current) and cached.
-unsigned char* noalloc_scratch()
+// looked up once per device (with that device current) and cached; `refresh`
+// looks it up again (after cudaDeviceReset the module, and with it the array,
+// is loaded anew and may sit elsewhere).  The lookup loads this file's device
+// module if it is not loaded yet (CUDA loads modules lazily by default), which
+// is when the array's memory is committed on the device.
+unsigned char* noalloc_scratch(bool refresh)
 {
     int dev = 0;
     GPUPR_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "device ordinal out of range"};
     std::lock_guard<std::mutex> lk(g_na_mu);
-    if (!g_na_ptr[dev]) {
+    if (!g_na_ptr[dev] || refresh) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            throw Error{GPUPR_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch) failed: ") +
-                                            cudaGetErrorString(e)};
+        if (e != cudaSuccess || !p) {
+            g_na_ptr[dev] = nullptr;
+            throw Error{e == cudaErrorMemoryAllocation ? GPUPR_ERR_OUT_OF_MEMORY : GPUPR_ERR_CUDA,
+                        std::string("cudaGetSymbolAddress(g_noalloc_scratch) failed: ") +
+                            cudaGetErrorString(e)};
+        }
         g_na_ptr[dev] = static_cast<unsigned char*>(p);
     }
     return g_na_ptr[dev];
@@ -1246,6 +1273,12 @@ const Ctl& read_ctl_stack(Ctl& h, const Ctl* d, cudaStream_t s)
 
 }  // namespace
 
+uint64_t noalloc_prepare()
+{
+    noalloc_scratch(true);
+    return (uint64_t)NA_BYTES;
+}
+
 void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t* d_term,
                            uint8_t* d_partition, const SolveOptions& opt, cudaStream_t s,
                            SolveResult& out)
@@ -1256,12 +1289,13 @@ void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t*
     if (n > NOALLOC_MAX_NODES)
         throw Error{GPUPR_ERR_INVALID_ARGUMENT,
                     "gpupr_solve_reduced_noalloc: n exceeds the static scratch limit of 1048576 nodes"};
-    unsigned char* base = noalloc_scratch();
+    unsigned char* base = noalloc_scratch(false);
     Ctl* ctl = reinterpret_cast<Ctl*>(base + NA_CTL);
     int32_t* err = reinterpret_cast<int32_t*>(base + NA_ERR);
     uint8_t* rev = base + NA_REV;
+    uint32_t* pair = reinterpret_cast<uint32_t*>(base + NA_PAIR);
     const int4* nbr = reinterpret_cast<const int4*>(d_nbr);
-    compute_reverse_slots_noalloc(n, nbr, rev, err, s);
+    compute_reverse_slots_noalloc(n, nbr, d_res, rev, pair, err, s);
     out.launches += 1;
 
     SolveView g{};
@@ -1269,6 +1303,7 @@ void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t*
     g.nbr = nbr;
     g.res = d_res;
     g.rev = rev;
+    g.pair = reinterpret_cast<const uint4*>(pair);
     g.term = d_term;
     g.excess = reinterpret_cast<long long*>(base + NA_EXCESS);
     g.height = reinterpret_cast<uint32_t*>(base + NA_HEIGHT);

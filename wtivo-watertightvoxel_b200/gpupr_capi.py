@@ -118,6 +118,7 @@ def lib():
         L.gpupr_surface_count.argtypes = [p, ctypes.c_int, p, u64, ctypes.c_int, p, p, u64, p, p, p]
         L.gpupr_surface_fetch.argtypes = [p, p, ctypes.c_int, p]
         L.gpupr_solve_reduced_noalloc.argtypes = [ctypes.c_uint32, p, p, p, p, i32, u64, i32, p, p]
+        L.gpupr_noalloc_prepare.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
         L.gpupr_graph_cut_batch.argtypes = [ctypes.c_uint32, p, p, p, ctypes.c_int, p, p, p,
                                             ctypes.c_int, f64, p, p, ctypes.c_int, p, p, p]
         L.gpupr_server_create.argtypes = [ctypes.c_uint64, ctypes.c_uint32, p, ctypes.POINTER(p)]
@@ -345,6 +346,28 @@ def solve_reduced(nbr, res, term, local_steps=8, global_relabel_period=1024, max
                                     _dp(exc) if exc is not None else None,
                                     _stream(torch, nbr.device), ctypes.byref(st)))
     return part[:n], st.as_dict(), exc
+
+
+def noalloc_prepare():
+    """gpupr_noalloc_prepare on the current device; returns the static
+    scratch array's size in bytes."""
+    nb = ctypes.c_uint64(0)
+    check(lib().gpupr_noalloc_prepare(ctypes.byref(nb)))
+    return int(nb.value)
+
+
+def solve_reduced_noalloc(nbr, res, term, part, local_steps=8, global_relabel_period=1024,
+                          max_rounds=2000000):
+    """gpupr_solve_reduced_noalloc on CUDA tensors (res/term modified in place,
+    the partition written to the uint8 CUDA tensor part).  Returns stats."""
+    import torch
+
+    st = CutStats()
+    check(lib().gpupr_solve_reduced_noalloc(int(nbr.shape[0]), _dp(nbr), _dp(res), _dp(term), _dp(part),
+                                            int(global_relabel_period), int(max_rounds),
+                                            int(local_steps), _stream(torch, nbr.device),
+                                            ctypes.byref(st)))
+    return st.as_dict()
 
 
 def solve_ell(nbr, cap, src, snk, opts=None):

@@ -68,6 +68,8 @@ def _L():
                                        ctypes.c_int64, p, ctypes.c_int64, p, p,
                                        ctypes.c_double, p]
         L.synth_udf_labels.restype = ctypes.c_int
+        L.synth_raw_graph.argtypes = [p, p, p, ctypes.c_int64, p, p, p, p, p]
+        L.synth_raw_graph.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -256,14 +258,40 @@ def proxy_points(V, F, n: int, eps: float, rng: np.random.Generator):
     return P
 
 
-def delaunay_cells(points):
+def delaunay_cells(points, spatial_order: bool = True):
     """Qhull Delaunay -> (tets int32 [N,4], neighbors int32 [N,4]) in the
-    CelloCut slot convention (slot fi = tet opposite local vertex 3-fi)."""
+    CelloCut slot convention (slot fi = tet opposite local vertex 3-fi).
+    With spatial_order the cells are renumbered in Morton order of their
+    centroids: CGAL inserts a point set in spatially sorted order, so its
+    cells come out spatially coherent, while Qhull's do not."""
     from scipy.spatial import Delaunay
-    d = Delaunay(np.asarray(points, np.float64))
+    P = np.asarray(points, np.float64)
+    d = Delaunay(P)
     tets = np.ascontiguousarray(d.simplices.astype(np.int32))
     nbrs = np.ascontiguousarray(d.neighbors[:, ::-1].astype(np.int32))
+    del d
+    if spatial_order:
+        tets, nbrs = morton_order_cells(P, tets, nbrs)
     return tets, nbrs
+
+
+def morton_order_cells(P, tets, nbrs, bits: int = 10):
+    """Cells renumbered by the Morton code of their centroids (stable)."""
+    cen = P[tets].mean(axis=1)
+    lo = cen.min(0)
+    span = np.maximum(cen.max(0) - lo, 1e-300)
+    q = np.clip(((cen - lo) / span * ((1 << bits) - 1)).astype(np.int64), 0, (1 << bits) - 1)
+    code = np.zeros(len(tets), np.int64)
+    for b in range(bits):
+        for a in range(3):
+            code |= ((q[:, a] >> b) & 1) << (3 * b + a)
+    order = np.argsort(code, kind="stable")
+    inv = np.empty(len(tets), np.int64)
+    inv[order] = np.arange(len(tets))
+    t2 = np.ascontiguousarray(tets[order])
+    n2 = nbrs[order]
+    n2 = np.where(n2 >= 0, inv[np.maximum(n2, 0)], -1).astype(np.int32)
+    return t2, np.ascontiguousarray(n2)
 
 
 def lattice_cells(shape, lo, hi, jitter: float = 0.15, seed: int = 0):
@@ -503,26 +531,22 @@ def config4(seed: int = 0, n_points: int = 2_000_000, use_delaunay: bool = True)
 def raw_graph_from_cells(P, tets, nbrs, rng):
     """Integer n-links round(1e4*area/mean_area), identical in both
     directions (each face's area is taken from its lower-id tet), and sphere
-    SDF t-links."""
-    lut = np.array([[0, 1, 2], [0, 1, 3], [0, 2, 3], [1, 2, 3]])
-    area = np.empty(tets.shape, np.float64)
-    for fi in range(4):
-        a, b, c = (P[tets[:, lut[fi, k]]] for k in range(3))
-        area[:, fi] = 0.5 * np.linalg.norm(np.cross(b - a, c - a), axis=1)
-    valid = nbrs >= 0
-    rev = _reverse_slots_np(nbrs)
-    i_idx = np.arange(len(tets))[:, None]
-    j = np.where(valid, nbrs, 0)
-    other = area[j, np.where(valid, rev, 0)]
-    face_area = np.where(i_idx <= j, area, other)
-    mean_area = float(area[valid].mean())
-    cap = np.where(valid, np.rint(1e4 * face_area / mean_area), 0).astype(np.int64)
-    cen = P[tets].mean(axis=1)
-    d = np.linalg.norm(cen - 0.5, axis=1) - 0.3 + rng.normal(scale=0.02, size=len(tets))
-    src = np.rint(100.0 * np.maximum(0.0, -d)).astype(np.int64)
-    snk = np.rint(100.0 * np.maximum(0.0, d)).astype(np.int64)
-    return dict(nbr=nbrs.astype(np.int32), cap=cap.astype(np.uint32), src=src.astype(np.uint32),
-                snk=snk.astype(np.uint32), n_points=len(P))
+    SDF t-links with Gaussian noise (sigma 0.02) drawn from rng
+    (synth_raw_graph in synth.c)."""
+    P = np.ascontiguousarray(P, np.float64)
+    tets = np.ascontiguousarray(tets, np.int32)
+    nbrs = np.ascontiguousarray(nbrs, np.int32)
+    N = len(tets)
+    noise = np.ascontiguousarray(rng.normal(scale=0.02, size=N))
+    scratch = np.empty((N, 4), np.float64)
+    cap = np.empty((N, 4), np.uint32)
+    src = np.empty(N, np.uint32)
+    snk = np.empty(N, np.uint32)
+    rc = _L().synth_raw_graph(_ptr(P), _ptr(tets), _ptr(nbrs), N, _ptr(noise), _ptr(scratch),
+                              _ptr(cap), _ptr(src), _ptr(snk))
+    if rc != 0:
+        raise ValueError("raw_graph_from_cells: asymmetric neighbours" if rc == -1 else "out of memory")
+    return dict(nbr=nbrs, cap=cap, src=src, snk=snk, n_points=len(P))
 
 
 def _reverse_slots_np(nbrs):

@@ -408,3 +408,79 @@ int synth_brick_udf(const double* MV, int64_t nv, const int32_t* MF, int64_t nf,
     }
     return bad ? -1 : 0;
 }
+
+/*
+ * synth_raw_graph: the integer-capacity raw graph of a tet mesh (all cells
+ * free, CelloCut slots).  n-link of slot k of tet i = rint(1e4 * area /
+ * mean_area), where area is the face's area taken from the face's lower-id
+ * tet, so both directions of a face carry the same capacity, and mean_area
+ * is the mean over every slot with a neighbour.  t-links from the signed
+ * distance of the centroid (mean of the 4 vertices) to the sphere of centre
+ * (0.5,0.5,0.5) and radius 0.3 plus noise[i]: src = rint(100 max(0, -d)),
+ * snk = rint(100 max(0, d)).  area_scratch holds 4N doubles.  Sums run over
+ * fixed blocks in a fixed order, so the result does not depend on the thread
+ * count.  Returns 0, or -1 when a neighbour does not list the tet back.
+ */
+int synth_raw_graph(const double* P, const int32_t* tets, const int32_t* nbrs, int64_t N,
+                    const double* noise, double* area_scratch, uint32_t* cap, uint32_t* src,
+                    uint32_t* snk)
+{
+    static const int lut[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+    const int64_t BLK = 65536;
+    const int64_t nblk = (N + BLK - 1) / BLK;
+    double* bsum = (double*)calloc((size_t)(nblk > 0 ? nblk : 1), sizeof(double));
+    int64_t* bcnt = (int64_t*)calloc((size_t)(nblk > 0 ? nblk : 1), sizeof(int64_t));
+    if (!bsum || !bcnt) { free(bsum); free(bcnt); return -2; }
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < nblk; ++b) {
+        double s = 0.0;
+        int64_t c = 0;
+        const int64_t e = (b + 1) * BLK < N ? (b + 1) * BLK : N;
+        for (int64_t i = b * BLK; i < e; ++i) {
+            for (int f = 0; f < 4; ++f) {
+                const double* a = P + 3 * (int64_t)tets[4 * i + lut[f][0]];
+                const double* q = P + 3 * (int64_t)tets[4 * i + lut[f][1]];
+                const double* r = P + 3 * (int64_t)tets[4 * i + lut[f][2]];
+                const double u0 = q[0] - a[0], u1 = q[1] - a[1], u2 = q[2] - a[2];
+                const double v0 = r[0] - a[0], v1 = r[1] - a[1], v2 = r[2] - a[2];
+                const double c0 = u1 * v2 - u2 * v1, c1 = u2 * v0 - u0 * v2, c2 = u0 * v1 - u1 * v0;
+                const double ar = 0.5 * sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+                area_scratch[4 * i + f] = ar;
+                if (nbrs[4 * i + f] >= 0) { s += ar; ++c; }
+            }
+        }
+        bsum[b] = s;
+        bcnt[b] = c;
+    }
+    double total = 0.0;
+    int64_t count = 0;
+    for (int64_t b = 0; b < nblk; ++b) { total += bsum[b]; count += bcnt[b]; }
+    free(bsum);
+    free(bcnt);
+    const double mean = count ? total / (double)count : 1.0;
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int64_t i = 0; i < N; ++i) {
+        for (int f = 0; f < 4; ++f) {
+            const int32_t j = nbrs[4 * i + f];
+            if (j < 0) { cap[4 * i + f] = 0u; continue; }
+            double fa = area_scratch[4 * i + f];
+            if ((int64_t)j < i) {
+                int rk = -1;
+                for (int k = 0; k < 4; ++k)
+                    if (nbrs[4 * (int64_t)j + k] == (int32_t)i) rk = k;
+                if (rk < 0) { bad = 1; rk = 0; }
+                fa = area_scratch[4 * (int64_t)j + rk];
+            }
+            cap[4 * i + f] = (uint32_t)rint(1e4 * fa / mean);
+        }
+        double c[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < 4; ++k)
+            for (int a = 0; a < 3; ++a) c[a] += P[3 * (int64_t)tets[4 * i + k] + a];
+        const double dx = 0.25 * c[0] - 0.5, dy = 0.25 * c[1] - 0.5, dz = 0.25 * c[2] - 0.5;
+        const double d = sqrt(dx * dx + dy * dy + dz * dz) - 0.3 + noise[i];
+        src[i] = (uint32_t)rint(100.0 * (d < 0.0 ? -d : 0.0));
+        snk[i] = (uint32_t)rint(100.0 * (d > 0.0 ? d : 0.0));
+    }
+    return bad ? -1 : 0;
+}
