@@ -72,7 +72,8 @@ WORKLOAD = "torus-knot (3,5) tube, 2% patches dropped, inner shell 0.002, noise 
 B_VISIT, B_PUSH, B_BFS = 73, 24, 57
 
 
-LEGS = ("e2e", "cpu", "batch", "serve", "labels", "audit", "raw", "config1", "noalloc", "autotune")
+LEGS = ("e2e", "cpu", "batch", "serve", "labels", "audit", "raw", "config1", "noalloc", "autotune",
+        "bottom_up")
 
 
 def parse():
@@ -454,6 +455,7 @@ def run_ours(args, world, rank, local):
     serve = run_serve(args) if "serve" in legs else None
     labels = run_labels(args, local, g) if "labels" in legs else None
     audit = run_audit(args, local, g, out, tets, nbrs) if "audit" in legs else None
+    bottom_up = run_bottom_up_ab(args, local, (V, tets, nbrs, L)) if "bottom_up" in legs else None
     del tets, nbrs, V, L, out
     torch.cuda.empty_cache()
     raw = run_raw(args, local) if "raw" in legs else None
@@ -482,7 +484,7 @@ def run_ours(args, world, rank, local):
                   "one_sweep_floor_ms": round(60.0 * s0["free_n"] / (pk["hbm_gbs"] * 1e9) * 1e3, 4)},
         "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
         "batch": batch, "serve": serve, "labels": labels, "audit": audit, "raw": raw,
-        "config1": config1, "noalloc": noalloc, "autotune": tune,
+        "config1": config1, "noalloc": noalloc, "bottom_up": bottom_up, "autotune": tune,
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
     }
     return line
@@ -716,6 +718,47 @@ def run_config1(args, local):
             "cpu_baseline": {"value": round(g.n_tets / cpu_s, 1), "unit": "tets/s", "cores": 1,
                              "kind": "port", "sample": "the whole graph: reduction + BK + scatter, "
                                                        "oracle/wtivo_oracle.c"}}
+
+
+def run_bottom_up_ab(args, local, bench_inputs):
+    """Direction-optimizing relabels, A/B: median device solve time of the
+    benchmark cut and of a 3M-tet holed-torus cut, relabels top-down only and
+    with bottom-up steps (switch when the unlabelled candidates number at most
+    ratio x the frontier; ratios 1 and 8), 5 alternating cuts per setting;
+    every setting's labels compared with the top-down cut's."""
+    import torch
+
+    import gpupr_capi
+    import synth
+
+    dev = torch.device("cuda", local)
+    tg = synth.config3_graph(1, 3_000_000, args.seed)
+    torus = tuple(torch.from_numpy(np.ascontiguousarray(tg[k])).to(dev)
+                  for k in ("vertices", "tets", "neighbors", "labels"))
+    settings = {"top_down": None,
+                "bottom_up_r1": gpupr_capi.options(bfs_bottom_up=1, bfs_bottom_up_ratio=1.0),
+                "bottom_up_r8": gpupr_capi.options(bfs_bottom_up=1, bfs_bottom_up_ratio=8.0)}
+    out = {}
+    for name, (V, T, Nb, L) in (("benchmark", bench_inputs), ("torus_3M", torus)):
+        lab = torch.empty(int(T.shape[0]), dtype=torch.uint8, device=dev)
+        ref = None
+        times = {k: [] for k in settings}
+        steps = {}
+        same = True
+        for rep in range(6):
+            for k, o in settings.items():
+                _, st = gpupr_capi.graph_cut(V, T, Nb, L, 10.0, out=lab, opts=o)
+                if rep:
+                    times[k].append(st["solve_device_ms"])
+                steps[k] = int(st["bottom_up_steps"])
+                if ref is None:
+                    ref = lab.clone()
+                else:
+                    same = same and bool(torch.equal(lab, ref))
+        out[name] = {"n_tets": int(T.shape[0]), "identical_cuts": same,
+                     **{k: {"solve_ms": round(float(np.median(v)), 3), "bottom_up_steps": steps[k]}
+                        for k, v in times.items()}}
+    return out
 
 
 def run_noalloc(args, local):

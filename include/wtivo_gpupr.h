@@ -20,8 +20,11 @@
 extern "C" {
 #endif
 
-#define GPUPR_ABI_VERSION 2   /* 2: stats and options carry the persistent engine's
-                                 grid, relabel factor and chaining; tuning entries */
+#define GPUPR_ABI_VERSION 3   /* 2: stats and options carry the persistent engine's
+                                 grid, relabel factor and chaining; tuning entries.
+                                 3: stats carry the active-sweep time, the graphs
+                                 a batch retired early and the bottom-up steps;
+                                 options carry the direction-optimizing BFS switch */
 
 typedef enum {
     GPUPR_OK = 0,
@@ -81,6 +84,11 @@ typedef struct {
     double relabel_work_factor; /* persistent engine: relabel work factor used */
     int64_t chain_hops;         /* persistent engine: chained discharge used */
     int64_t chain_max_active;
+    double sweep_ms;            /* persistent engine: active sweeps after each relabel
+                                   (part of bfs_ms) */
+    uint64_t graphs_retired;    /* batch: graphs finished and left out of the
+                                   relabels before the last one */
+    uint64_t bottom_up_steps;   /* BFS steps run bottom-up (bfs_bottom_up) */
 } gpupr_cut_stats;
 
 /* Solver tuning knobs; zero fields take the defaults shown. */
@@ -113,6 +121,13 @@ typedef struct {
                                      active nodes (default by graph size: 131072
                                      below 1.5M free nodes, 32768 below 2M,
                                      else 4096) */
+    int32_t bfs_bottom_up;        /* persistent engine: 1 = direction-optimizing
+                                     global relabels (bottom-up steps over the
+                                     nodes the previous relabel reached and this
+                                     one has not, once they number at most
+                                     bfs_bottom_up_ratio x the frontier);
+                                     0 = top-down only (default) */
+    double bfs_bottom_up_ratio;   /* default 1 */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

@@ -19,7 +19,7 @@ def test_library_exports_header(built):
     L = ctypes.CDLL(str(gpupr_capi.LIB_PATH))
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
-    assert gpupr_capi.lib().gpupr_abi_version() == 2
+    assert gpupr_capi.lib().gpupr_abi_version() == 3
     assert gpupr_capi.lib().gpupr_status_string(9) == b"GPUPr-FAST-v6.30 max macro rounds exceeded"
 
 
@@ -139,3 +139,30 @@ def test_tune_table_round_trip(built, tmp_path):
             gpupr_capi.set_tune_table([bad])
     assert gpupr_capi.tune_table() == entries        # a rejected set changes nothing
     gpupr_capi.set_tune_table([])
+
+
+def test_python_structs_match_the_header(tmp_path):
+    """The ctypes mirrors of the C structs have the header's size and field
+    offsets (checked with a C program compiled against include/wtivo_gpupr.h)."""
+    import subprocess
+
+    import gpupr_capi
+
+    checks = {"gpupr_cut_stats": gpupr_capi.CutStats, "gpupr_solve_options": gpupr_capi.SolveOptions,
+              "gpupr_batch_item": gpupr_capi.BatchItem, "gpupr_request_result": gpupr_capi.RequestResult,
+              "gpupr_tune_entry": gpupr_capi.TuneEntry, "gpupr_brick_grid": gpupr_capi.BrickGrid}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "wtivo_gpupr.h"', "int main(void) {"]
+    for cname, py in checks.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "sizes.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "sizes"
+    subprocess.check_call(["gcc", "-I", str(gpupr_capi.HEADER.parent), str(src), "-o", str(exe)])
+    got = dict(line.split() for line in subprocess.check_output([str(exe)], text=True).splitlines())
+    for cname, py in checks.items():
+        assert int(got[cname]) == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, (cname, f)

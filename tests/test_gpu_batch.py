@@ -28,12 +28,13 @@ def _run_batch(graphs, **kw):
     return toff, gpupr_capi.graph_cut_batch(toff, voff, V, t, n, L, 10.0, **kw)
 
 
-@pytest.mark.parametrize("engine", [1, 2])
-def test_batch_equals_individual_cuts(built, engine):
+@pytest.mark.parametrize("engine,bottom_up", [(1, 0), (2, 0), (2, 1)])
+def test_batch_equals_individual_cuts(built, engine, bottom_up):
     import gpupr_capi
 
     graphs = _graphs()
-    toff, (out, items, st) = _run_batch(graphs, opts=gpupr_capi.options(engine=engine))
+    toff, (out, items, st) = _run_batch(graphs, opts=gpupr_capi.options(
+        engine=engine, bfs_bottom_up=bottom_up, bfs_bottom_up_ratio=1e9 if bottom_up else 0.0))
     assert len(items) == len(graphs)
     for k, g in enumerate(graphs):
         lab, ost = orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0)
@@ -77,3 +78,17 @@ def test_batch_device_resident_and_repeatable(built):
     o1, it1, _ = gpupr_capi.graph_cut_batch(toff, voff, v, t, n, l, 10.0)
     o2, it2, _ = gpupr_capi.graph_cut_batch(toff, voff, V, t, n, L, 10.0)
     assert np.array_equal(o1.cpu().numpy(), o2) and it1 == it2
+
+
+def test_batch_retires_finished_graphs(built):
+    """Graphs of very different size finish at different relabels: the small
+    ones retire while the large one still runs, and every graph keeps exactly
+    its own cut (its labels from the relabel at which it retired)."""
+    graphs = [cached_graph("lattice", 2, 80_000)] + [cached_graph("proxy", s, 6_000) for s in range(6)] + \
+             [cached_graph("lattice", 3, 300_000)]
+    toff, (out, items, st) = _run_batch(graphs)
+    assert st["engine"] == 2 and st["graphs_retired"] >= 1
+    for k, g in enumerate(graphs):
+        lab, ost = orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0)
+        assert np.array_equal(out[int(toff[k]):int(toff[k + 1])], lab), k
+        assert items[k]["adjusted_flow"] == ost["adjusted_flow"], k

@@ -215,6 +215,9 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
     st->relabel_work_factor = sr.work_factor;
     st->chain_hops = sr.chain_hops;
     st->chain_max_active = sr.chain_max_active;
+    st->sweep_ms = sr.sweep_ms;
+    st->graphs_retired = sr.graphs_retired;
+    st->bottom_up_steps = sr.bottom_up_steps;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -402,9 +405,30 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
         opt.chain_max_active = 131072;
         opt.blocks_per_sm = 3;
     }
+    // each graph's free nodes form one contiguous range of reduced ids: the
+    // segments of the solve (per-graph retirement) and of the per-graph flows
+    DevBuf<unsigned long long> counts(G, s), d_foff(G + 1, s), base(G, s);
+    DevBuf<uint32_t> d_soff(G + 1, s);
+    DevBuf<long long> raw(G, s);
+    batch_free_counts(G, d_toff.p, g.full_to_free.p, counts.p, s, &launches);
+    std::vector<unsigned long long> hc(G), hfo(G + 1), hb(G);
+    std::vector<uint32_t> hso(G + 1);
+    std::vector<long long> hr(G);
+    GPUPR_CUDA(cudaMemcpyAsync(hc.data(), counts.p, G * 8u, cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    hfo[0] = 0;
+    for (uint32_t k = 0; k < G; ++k) hfo[k + 1] = hfo[k] + hc[k];
+    if (hfo[G] != g.n) throw Error{GPUPR_ERR_INVARIANT, "batch free counts do not add up"};
+    for (uint32_t k = 0; k <= G; ++k) hso[k] = (uint32_t)hfo[k];
+    GPUPR_CUDA(cudaMemcpyAsync(d_foff.p, hfo.data(), (G + 1) * 8u, cudaMemcpyHostToDevice, s));
+    GPUPR_CUDA(cudaMemcpyAsync(d_soff.p, hso.data(), (G + 1) * 4u, cudaMemcpyHostToDevice, s));
+    Segments segs;
+    segs.nseg = G;
+    segs.d_off = d_soff.p;
+
     SolveWorkspace w;
     SolveResult sr;
-    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr);
+    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr, &segs);
     launches += sr.launches;
 
     DevBuf<uint8_t> dout;
@@ -417,16 +441,6 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     scatter_partition(g.n, g.free_old.p, w.height.p, d_out, s, &launches);
 
     // per-graph flows over each graph's contiguous free-node range
-    DevBuf<unsigned long long> counts(G, s), d_foff(G + 1, s), base(G, s);
-    DevBuf<long long> raw(G, s);
-    batch_free_counts(G, d_toff.p, g.full_to_free.p, counts.p, s, &launches);
-    std::vector<unsigned long long> hc(G), hfo(G + 1), hb(G);
-    std::vector<long long> hr(G);
-    GPUPR_CUDA(cudaMemcpyAsync(hc.data(), counts.p, G * 8u, cudaMemcpyDeviceToHost, s));
-    GPUPR_CUDA(cudaStreamSynchronize(s));
-    hfo[0] = 0;
-    for (uint32_t k = 0; k < G; ++k) hfo[k + 1] = hfo[k] + hc[k];
-    GPUPR_CUDA(cudaMemcpyAsync(d_foff.p, hfo.data(), (G + 1) * 8u, cudaMemcpyHostToDevice, s));
     batch_flows(G, d_foff.p, g.term.p, w.excess.p, g.base_node.p, raw.p, base.p, s, &launches);
     GPUPR_CUDA(cudaMemcpyAsync(hr.data(), raw.p, G * 8u, cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaMemcpyAsync(hb.data(), base.p, G * 8u, cudaMemcpyDeviceToHost, s));
@@ -459,6 +473,9 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     st->relabel_work_factor = sr.work_factor;
     st->chain_hops = sr.chain_hops;
     st->chain_max_active = sr.chain_max_active;
+    st->sweep_ms = sr.sweep_ms;
+    st->graphs_retired = sr.graphs_retired;
+    st->bottom_up_steps = sr.bottom_up_steps;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -669,6 +686,9 @@ gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_r
             stats->relabel_work_factor = sr.work_factor;
             stats->chain_hops = sr.chain_hops;
             stats->chain_max_active = sr.chain_max_active;
+            stats->sweep_ms = sr.sweep_ms;
+            stats->graphs_retired = sr.graphs_retired;
+            stats->bottom_up_steps = sr.bottom_up_steps;
             stats->kernel_launches = launches;
         }
     });
@@ -731,6 +751,9 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
             stats->relabel_work_factor = sr.work_factor;
             stats->chain_hops = sr.chain_hops;
             stats->chain_max_active = sr.chain_max_active;
+            stats->sweep_ms = sr.sweep_ms;
+            stats->graphs_retired = sr.graphs_retired;
+            stats->bottom_up_steps = sr.bottom_up_steps;
             stats->kernel_launches = launches;
         }
     });

@@ -40,8 +40,26 @@ struct Ctl {
     uint32_t pad0;
     // persistent engine, globaltimer ns of block 0 summed per phase: BFS
     // (seed + steps), active sweeps, discharge rounds
-    unsigned long long bfs_ns, sweep_ns, discharge_ns, pad1;
+    unsigned long long bfs_ns, sweep_ns, discharge_ns;
+    // segmented solves: graphs retired (no active node after an exact
+    // relabel) and their free nodes
+    unsigned long long retired_nodes;
+    uint32_t segs_retired;
+    // direction-optimizing relabels: the reached set the active sweep collects
+    // for the next relabel, its size in the current relabel, nodes first
+    // labelled per BFS step (ring by level, like bfs_cnt), sizes of the
+    // bottom-up candidate lists (ring by bottom-up step), bottom-up steps run
+    uint32_t cand_build;
+    uint32_t cand_cnt;
+    uint32_t lab_cnt[3];
+    uint32_t bu_cnt[3];
+    uint32_t bu_steps;
 };
+
+// Nodes per pass of a whole-array sweep (seed, excess init, active sweep):
+// 256 threads x 4 nodes.  Segmented solves keep the first graph of every such
+// chunk.
+constexpr uint32_t SWEEP_CHUNK = 1024u;
 
 constexpr unsigned long long BAR_ABORT = 1ull << 62;
 constexpr unsigned long long BAR_COUNT = (1ull << 40) - 1;
@@ -68,6 +86,18 @@ struct SolveView {
     uint32_t chain_max_active;          // ... in rounds of at most this many nodes
     int bfs_hops;                       // nodes one thread may label in a row in one
                                         // short BFS step (<= 1: level by level)
+    // Segmented solve (a batch: independent graphs, each a contiguous node
+    // range; persistent engine).  nseg == 0: one graph.
+    uint32_t nseg;
+    const uint32_t* __restrict__ seg_off;    // [nseg+1] first node of each graph
+    const uint32_t* __restrict__ chunk_seg;  // [ceil(n/SWEEP_CHUNK)] first graph of each chunk
+    uint32_t* seg_live;                 // [nseg] nonzero while the graph is being solved
+    uint32_t* seg_act;                  // [nseg] the last active sweep found an active node
+    // Direction-optimizing relabels (persistent engine): candidate lists of
+    // n entries each, and the switch ratio (bottom_up == 0: top-down only)
+    uint32_t* cand[2];
+    int bottom_up;
+    float bu_ratio;
 };
 
 // ---------------------------------------------------------------------------
@@ -228,6 +258,8 @@ struct SolveOptions {
     int engine = 0;                // 0 auto, 1 one launch per step, 2 persistent
     int chain_hops = 0;            // persistent engine: 0 = default
     int chain_max_active = 0;      // persistent engine: 0 = default
+    int bfs_bottom_up = 0;         // persistent engine: direction-optimizing relabels
+    double bfs_bottom_up_ratio = 1.0;
 };
 
 SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw,
@@ -238,10 +270,20 @@ struct SolveWorkspace {
     DevBuf<uint32_t> height;
     DevBuf<uint32_t> q0, q1, q2;
     DevBuf<Ctl> ctl;
+    DevBuf<uint32_t> chunk_seg, seg_live, seg_act;   // segmented solves only
+    DevBuf<uint32_t> cand0, cand1;                   // direction-optimizing relabels only
     uint64_t bytes() const
     {
-        return excess.bytes() + height.bytes() + q0.bytes() + q1.bytes() + q2.bytes() + ctl.bytes();
+        return excess.bytes() + height.bytes() + q0.bytes() + q1.bytes() + q2.bytes() + ctl.bytes() +
+               chunk_seg.bytes() + seg_live.bytes() + seg_act.bytes() + cand0.bytes() + cand1.bytes();
     }
+};
+
+// The graphs of a batch as node ranges of the reduced union graph: graph k
+// owns reduced ids [d_off[k], d_off[k+1]) (device, nseg + 1 entries).
+struct Segments {
+    uint32_t nseg = 0;
+    const uint32_t* d_off = nullptr;
 };
 
 struct SolveResult {
@@ -252,6 +294,8 @@ struct SolveResult {
     double discharge_ms = 0.0, bfs_ms = 0.0, sweep_ms = 0.0;
     uint64_t discharge_launches = 0, bfs_launches = 0;
     uint64_t workspace_bytes = 0;
+    uint64_t graphs_retired = 0;   // segmented solves: graphs finished before the last relabel
+    uint64_t bottom_up_steps = 0;  // BFS steps run bottom-up
     int engine = 1;                // 1 one launch per step, 2 persistent
     int blocks_per_sm = 0;         // persistent engine: grid used
     double work_factor = 0.0;      // persistent engine: relabel work factor used
@@ -274,9 +318,13 @@ int size_class(uint32_t n);
 // Phase-I push-relabel on a reduced graph (res/term updated in place).
 // On return the workspace heights mark the sink-reachable set
 // (height != UNVIS) of the final residual graph.
+// With segments (a batch), the persistent engine retires each graph once an
+// exact relabel finds no active node in it; the one-launch-per-step engine
+// solves the union as one graph.
 void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const uint8_t* d_rev,
                         const uint32_t* d_pair, int32_t* d_term, SolveWorkspace& w,
-                        const SolveOptions& opt, cudaStream_t s, SolveResult& out);
+                        const SolveOptions& opt, cudaStream_t s, SolveResult& out,
+                        const Segments* segments = nullptr);
 
 // Cut-surface extraction (surface.cu): count keeps its result per thread
 // for the following fetch.

@@ -41,6 +41,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <chrono>
 #include <mutex>
 #include <cmath>
@@ -56,6 +57,11 @@ constexpr int DTPB = 256;   // block size of the solver kernels
 __device__ __forceinline__ uint32_t ldcg(const uint32_t* p) { return __ldcg(p); }
 __device__ __forceinline__ int32_t ldcg(const int32_t* p) { return __ldcg(p); }
 __device__ __forceinline__ long long ldcg(const long long* p) { return __ldcg(p); }
+
+// A load that bypasses the caches' stale copies (control counters written by
+// other blocks before the last grid barrier).
+template <class T>
+__device__ __forceinline__ T vload(const T* p) { return *reinterpret_cast<const volatile T*>(p); }
 
 template <class T>
 __device__ __forceinline__ T warp_block_sum(T v, T* sh)
@@ -112,6 +118,26 @@ constexpr uint32_t BFS_EAGER_MAX = 32768u;
 // many independent loads in flight per thread make the pass stream instead
 // of waiting for one round trip per node.
 constexpr int SWEEP_UNROLL = 4;
+static_assert(DTPB * SWEEP_UNROLL == (int)SWEEP_CHUNK, "sweep chunk of the segment table");
+
+// The graph of node v in a segmented solve, searched forward from seg (the
+// first graph of v's sweep chunk; graphs without nodes are stepped over).
+__device__ __forceinline__ uint32_t seg_of(const SolveView& g, uint32_t seg, uint32_t v)
+{
+    while (seg + 1u < g.nseg && __ldg(g.seg_off + seg + 1u) <= v) ++seg;
+    return seg;
+}
+
+// Whether a sweep handles node v: every node of a single graph; in a
+// segmented solve only nodes of graphs not yet retired.  *seg: v's graph.
+__device__ __forceinline__ bool sweep_node(const SolveView& g, uint32_t seg0, uint32_t v, uint32_t* seg)
+{
+    *seg = 0u;
+    if (v >= g.n) return false;
+    if (!g.nseg) return true;
+    *seg = seg_of(g, seg0, v);
+    return ldcg(g.seg_live + *seg) != 0u;
+}
 
 // Level 1 of the backward BFS: nodes with a residual arc to the sink.  Every
 // other height is reset to UNVIS (.cu:374-379).  s_m[0..5] are the block's
@@ -126,23 +152,27 @@ __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr
     Ctl* ctl = g.ctl;
     constexpr uint32_t CH = DTPB * SWEEP_UNROLL;
     for (uint32_t base = blockIdx.x * CH; base < g.n; base += gridDim.x * CH) {
+        const uint32_t seg0 = g.nseg ? __ldg(g.chunk_seg + base / CH) : 0u;
+        bool in[SWEEP_UNROLL];
         int32_t t[SWEEP_UNROLL];
 #pragma unroll
         for (int j = 0; j < SWEEP_UNROLL; ++j) {
             const uint32_t v = base + j * DTPB + threadIdx.x;
-            t[j] = v < g.n ? ldcg(g.term + v) : 0;
+            uint32_t sg;
+            in[j] = sweep_node(g, seg0, v, &sg);   // a retired graph keeps its labels
+            t[j] = in[j] ? ldcg(g.term + v) : 0;
         }
         long long x[SWEEP_UNROLL];
 #pragma unroll
         for (int j = 0; j < SWEEP_UNROLL; ++j) {
             const uint32_t v = base + j * DTPB + threadIdx.x;
-            x[j] = (kActive && v < g.n && t[j] < 0) ? ldcg(g.excess + v) : 0ll;
-            if (v < g.n) g.height[v] = (t[j] < 0) ? 1u : UNVIS;
+            x[j] = (kActive && in[j] && t[j] < 0) ? ldcg(g.excess + v) : 0ll;
+            if (in[j]) g.height[v] = (t[j] < 0) ? 1u : UNVIS;
         }
 #pragma unroll
         for (int j = 0; j < SWEEP_UNROLL; ++j) {
             const uint32_t v = base + j * DTPB + threadIdx.x;
-            if (v < g.n && t[j] < 0) {
+            if (in[j] && t[j] < 0) {
                 s_fr[atomicAdd(&s_m[0], 1u)] = v;
                 if (kActive && 1u < g.n && x[j] > 0) s_act[atomicAdd(&s_m[1], 1u)] = v;
             }
@@ -152,6 +182,7 @@ __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr
             s_m[2] = s_m[0]; s_m[3] = s_m[1]; s_m[0] = 0; s_m[1] = 0;
             s_m[4] = s_m[2] ? atomicAdd(&ctl->bfs_cnt[1], s_m[2]) : 0u;
             s_m[5] = s_m[3] ? atomicAdd(&ctl->act_cnt[0], s_m[3]) : 0u;
+            if (g.bottom_up && s_m[2]) atomicAdd(&ctl->lab_cnt[1], s_m[2]);
         }
         __syncthreads();
         flush_stage(s_fr, s_m[2], s_m[4], g.fr[1], g.n, ctl);
@@ -188,30 +219,48 @@ __device__ __forceinline__ uint32_t queue_index(uint32_t it, uint32_t cnt)
 // label below n and positive excess, appended in node order by one streaming
 // pass (12 bytes a node) instead of a random excess load for each node the
 // BFS labels.  s_act holds DTPB * SWEEP_UNROLL entries; s_m[1], s_m[3] and
-// s_m[5] are its staging counters.
-__device__ __forceinline__ void active_sweep_body(const SolveView& g, uint32_t* s_act, uint32_t* s_m)
+// s_m[5] are its staging counters.  In a segmented solve it also marks the
+// graphs that still hold an active node.  With direction-optimizing relabels
+// the same pass collects every reached node (label below UNVIS) into
+// cand[0], staged in s_cand (DTPB * SWEEP_UNROLL entries, counters
+// s_m[7..9]): the candidates of the next relabel's bottom-up steps.
+__device__ __forceinline__ void active_sweep_body(const SolveView& g, uint32_t* s_act, uint32_t* s_cand,
+                                                  uint32_t* s_m)
 {
     Ctl* ctl = g.ctl;
     constexpr uint32_t CH = DTPB * SWEEP_UNROLL;
     for (uint32_t base = blockIdx.x * CH; base < g.n; base += gridDim.x * CH) {
-        uint32_t h[SWEEP_UNROLL];
+        const uint32_t seg0 = g.nseg ? __ldg(g.chunk_seg + base / CH) : 0u;
+        uint32_t h[SWEEP_UNROLL], sg[SWEEP_UNROLL];
         long long x[SWEEP_UNROLL];
 #pragma unroll
         for (int j = 0; j < SWEEP_UNROLL; ++j) {
             const uint32_t v = base + j * DTPB + threadIdx.x;
-            h[j] = v < g.n ? ldcg(g.height + v) : UNVIS;
-            x[j] = v < g.n ? ldcg(g.excess + v) : 0ll;
+            const bool in = sweep_node(g, seg0, v, &sg[j]);
+            h[j] = in ? ldcg(g.height + v) : UNVIS;
+            x[j] = in ? ldcg(g.excess + v) : 0ll;
         }
 #pragma unroll
-        for (int j = 0; j < SWEEP_UNROLL; ++j)
-            if (h[j] < g.n && x[j] > 0) s_act[atomicAdd(&s_m[1], 1u)] = base + j * DTPB + threadIdx.x;
+        for (int j = 0; j < SWEEP_UNROLL; ++j) {
+            const bool act = h[j] < g.n && x[j] > 0;
+            if (act) s_act[atomicAdd(&s_m[1], 1u)] = base + j * DTPB + threadIdx.x;
+            if (g.bottom_up && h[j] != UNVIS) s_cand[atomicAdd(&s_m[7], 1u)] = base + j * DTPB + threadIdx.x;
+            if (g.nseg) {
+                // the graph still has work: one store per group of lanes in the same graph
+                const unsigned grp = __match_any_sync(0xffffffffu, act ? sg[j] : 0xFFFFFFFFu);
+                if (act && (int)(threadIdx.x & 31u) == __ffs(grp) - 1) g.seg_act[sg[j]] = 1u;
+            }
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
             s_m[3] = s_m[1]; s_m[1] = 0;
             s_m[5] = s_m[3] ? atomicAdd(&ctl->act_cnt[0], s_m[3]) : 0u;
+            s_m[8] = s_m[7]; s_m[7] = 0;
+            s_m[9] = s_m[8] ? atomicAdd(&ctl->cand_build, s_m[8]) : 0u;
         }
         __syncthreads();
         flush_stage(s_act, s_m[3], s_m[5], g.act[0], g.n, ctl);
+        if (g.bottom_up) flush_stage(s_cand, s_m[8], s_m[9], g.cand[0], g.n, ctl);
         __syncthreads();
     }
 }
@@ -429,6 +478,7 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
                     const int v = nb[k];
                     if (!((arcs >> k) & 1u) || hv[k] <= cand) continue;
                     const uint32_t old = atomicMin(g.height + v, cand);
+                    if (g.bottom_up && old == UNVIS) atomicAdd(&s_m[6], 1u);   // a first label
                     if (old <= cand || (old != UNVIS && !propagate)) continue;
                     if (hop < hops && next == UNVIS) next = (uint32_t)v;
                     else stage_push(g, sf, (uint32_t)v);
@@ -443,9 +493,73 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
             s_m[2] = min(s_m[0], stage_cap);
             s_m[0] = 0;
             s_m[4] = s_m[2] ? atomicAdd(gcnt, s_m[2]) : 0u;
+            if (g.bottom_up && s_m[6]) {
+                atomicAdd(&ctl->lab_cnt[(L + 1) % 3], s_m[6]);
+                s_m[6] = 0;
+            }
         }
         __syncthreads();
         flush_stage(s_fr, s_m[2], s_m[4], out, g.n, ctl);
+        __syncthreads();
+    }
+}
+
+// One bottom-up step j of a direction-optimizing relabel (frontier label L):
+// every candidate v of list j (cand[j % 2], size in bu_cnt[j % 3]; list 0 is
+// the previous relabel's reached set, which holds every node this relabel can
+// reach: a push runs only between reached nodes, so the reached set never
+// grows) that is still unlabelled and has a residual arc to a labelled
+// neighbour takes 1 + the lowest such label and joins the next frontier;
+// the others stay candidates in list j+1.  v's own rows give the arcs v->u,
+// so only the neighbours' labels are gathered.  s_fr and s_keep hold
+// stage_cap entries each; s_m[0,2,4] stage the frontier, s_m[7..9] the list.
+__device__ __forceinline__ void bfs_bottom_up_body(const SolveView& g, uint32_t L, uint32_t j,
+                                                   uint32_t* s_fr, uint32_t* s_keep, uint32_t stage_cap,
+                                                   uint32_t* s_m, unsigned long long& visits)
+{
+    Ctl* ctl = g.ctl;
+    const uint32_t* in = g.cand[j & 1u];
+    uint32_t* keep = g.cand[(j + 1u) & 1u];
+    uint32_t* kcnt = &ctl->bu_cnt[(j + 1u) % 3u];
+    uint32_t* out = (L & 1) ? g.fr[0] : g.fr[1];
+    uint32_t* gcnt = &ctl->bfs_cnt[(L + 1) % 3];
+    const uint32_t cnt = min(vload(&ctl->bu_cnt[j % 3u]), g.n);
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->bu_cnt[(j + 2u) % 3u] = 0u;
+    for (uint32_t it = 0; it * (gridDim.x * DTPB) < cnt; ++it) {
+        const uint32_t i = (it * gridDim.x + blockIdx.x) * DTPB + threadIdx.x;   // node order
+        if (i < cnt) {
+            const uint32_t v = __ldcg(in + i);
+            if (v < g.n && ldcg(g.height + v) == UNVIS) {
+                const int4 nb4 = __ldg(g.nbr + v);
+                const uint4 r4 = __ldcg(reinterpret_cast<const uint4*>(g.res) + v);
+                const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+                const uint32_t r[4] = {r4.x, r4.y, r4.z, r4.w};
+                uint32_t hv[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) hv[k] = (nb[k] >= 0 && r[k] != 0u) ? ldcg(g.height + nb[k]) : UNVIS;
+                const uint32_t best = min(min(hv[0], hv[1]), min(hv[2], hv[3]));
+                ++visits;
+                if (best != UNVIS) {
+                    atomicMin(g.height + v, best + 1u);
+                    s_fr[atomicAdd(&s_m[0], 1u)] = v;
+                } else {
+                    s_keep[atomicAdd(&s_m[7], 1u)] = v;
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_m[2] = min(s_m[0], stage_cap);
+            s_m[0] = 0;
+            s_m[4] = s_m[2] ? atomicAdd(gcnt, s_m[2]) : 0u;
+            if (s_m[2]) atomicAdd(&ctl->lab_cnt[(L + 1) % 3], s_m[2]);
+            s_m[8] = min(s_m[7], stage_cap);
+            s_m[7] = 0;
+            s_m[9] = s_m[8] ? atomicAdd(kcnt, s_m[8]) : 0u;
+        }
+        __syncthreads();
+        flush_stage(s_fr, s_m[2], s_m[4], out, g.n, ctl);
+        flush_stage(s_keep, s_m[8], s_m[9], keep, g.n, ctl);
         __syncthreads();
     }
 }
@@ -622,6 +736,26 @@ __global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
 // follow the same path.  Every barrier wait is bounded; an error or the time
 // limit makes every block leave at its next barrier.
 // ---------------------------------------------------------------------------
+// Segmented solve: a graph in which the active sweep after an exact relabel
+// found no active node is finished (its preflow is maximum and nothing in it
+// changes any more), so it retires: the seeds and sweeps that follow skip its
+// nodes, no BFS enters it (the graphs share no arc), and its labels from this
+// relabel give its partition.  Clears the marks of the graphs that go on.
+__device__ __forceinline__ void retire_graphs(const SolveView& g)
+{
+    for (uint32_t k = blockIdx.x * DTPB + threadIdx.x; k < g.nseg; k += gridDim.x * DTPB) {
+        if (!ldcg(g.seg_live + k)) continue;
+        if (ldcg(g.seg_act + k)) {
+            g.seg_act[k] = 0u;
+            continue;
+        }
+        g.seg_live[k] = 0u;
+        atomicAdd(&g.ctl->segs_retired, 1u);
+        atomicAdd(&g.ctl->retired_nodes,
+                  (unsigned long long)(__ldg(g.seg_off + k + 1u) - __ldg(g.seg_off + k)));
+    }
+}
+
 struct PersistParams {
     unsigned long long max_rounds;
     unsigned long long budget;      // node visits per discharge phase, 0 = none
@@ -636,9 +770,6 @@ __device__ __forceinline__ unsigned long long gtimer()
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-
-template <class T>
-__device__ __forceinline__ T vload(const T* p) { return *reinterpret_cast<const volatile T*>(p); }
 
 __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p)
 {
@@ -693,7 +824,7 @@ __device__ bool grid_barrier(Ctl* ctl, unsigned long long& target, unsigned long
 __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, PersistParams p)
 {
     __shared__ uint32_t s_buf[DTPB * 8];
-    __shared__ uint32_t s_m[8];
+    __shared__ uint32_t s_m[12];
     __shared__ unsigned long long s_red[DTPB / 32];
     __shared__ int s_ok;
     Ctl* ctl = g.ctl;
@@ -702,6 +833,7 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
     unsigned long long bar_target = 0;
     Work w;
     unsigned long long bfs_visits = 0;
+    if (threadIdx.x < 12) s_m[threadIdx.x] = 0u;
     // phase clock of block 0, read after each phase's closing barrier:
     // s_clk = {BFS, active sweep, discharge, last mark} (shared memory, so it
     // holds no registers through the solve)
@@ -713,7 +845,6 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
             s_clk[3] = t;
         }
     };
-    if (threadIdx.x == 0) { s_m[0] = 0; s_m[1] = 0; }
     constexpr uint32_t CH = DTPB * SWEEP_UNROLL;
     for (uint32_t base = blockIdx.x * CH; base < g.n; base += gridDim.x * CH) {
         int32_t t[SWEEP_UNROLL];
@@ -739,20 +870,37 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
             uint32_t L = 1;
             bool exact = true;   // no chained step yet: every frontier node is labelled L
+            uint32_t labelled = 0, bu_j = 0;
             for (;;) {
                 const uint32_t first = prefetch_entry((L & 1) ? g.fr[1] : g.fr[0], g.n);
                 const uint32_t cnt = min(vload(&ctl->bfs_cnt[L % 3]), g.n);
                 if (cnt == 0) break;
                 if (lead) ctl->bfs_cnt[(L + 2) % 3] = 0u;
-                // the same decision in every block: it depends on cnt alone
-                const unsigned long long nn = g.n;
-                const int hops = (g.bfs_hops > 1 && cnt <= SPREAD_MAX &&
-                                  4ull * (unsigned long long)g.bfs_hops * cnt <= nn)
-                                     ? g.bfs_hops : 1;
-                const bool propagate = 4ull * (unsigned long long)hops * cnt <= nn;
-                bfs_step_body(g, L, cnt, first, s_buf, DTPB * 8, s_m, bfs_visits, hops, propagate,
-                              exact);
-                if (hops > 1) exact = false;
+                // every decision below is the same in every block: it depends
+                // on counters completed before the last barrier
+                bool bottom_up = false;
+                if (g.bottom_up) {
+                    labelled += vload(&ctl->lab_cnt[L % 3]);
+                    if (lead) ctl->lab_cnt[(L + 2) % 3] = 0u;
+                    const uint32_t cc = vload(&ctl->cand_cnt);
+                    const uint32_t rem = cc > labelled ? cc - labelled : 0u;
+                    bottom_up = cc != 0u && (float)rem <= g.bu_ratio * (float)cnt;
+                }
+                if (bottom_up) {
+                    bfs_bottom_up_body(g, L, bu_j, s_buf, s_buf + DTPB * 4, DTPB * 4, s_m, bfs_visits);
+                    ++bu_j;
+                    exact = false;
+                    if (lead) ++ctl->bu_steps;
+                } else {
+                    const unsigned long long nn = g.n;
+                    const int hops = (g.bfs_hops > 1 && cnt <= SPREAD_MAX &&
+                                      4ull * (unsigned long long)g.bfs_hops * cnt <= nn)
+                                         ? g.bfs_hops : 1;
+                    const bool propagate = 4ull * (unsigned long long)hops * cnt <= nn;
+                    bfs_step_body(g, L, cnt, first, s_buf, DTPB * 8, s_m, bfs_visits, hops, propagate,
+                                  exact);
+                    if (hops > 1) exact = false;
+                }
                 if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
                 ++L;
                 ++levels_total;
@@ -765,13 +913,15 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
             if (!ok) break;
             ++relabels;
             lap(0);
-            active_sweep_body(g, s_buf, s_m);
+            active_sweep_body(g, s_buf, s_buf + DTPB * 4, s_m);
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
             lap(1);
             if (vload(&ctl->act_cnt[0]) == 0u) break;   // maximum preflow
+            if (g.nseg) retire_graphs(g);
             // ---- discharge rounds ----
             uint32_t r = 0;
             unsigned long long visits = 0;
+            unsigned long long budget = p.budget;
             for (;;) {
                 const uint32_t first = prefetch_entry((r & 1) ? g.act[1] : g.act[0], g.n);
                 const uint32_t cnt = min(vload(&ctl->act_cnt[r % 3]), g.n);
@@ -787,12 +937,28 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
                 ++r;
                 ++rounds_total;
                 visits += cnt;
+                if (g.nseg && r == 1u && budget) {
+                    // the work between relabels follows the nodes still being
+                    // solved (read after a barrier that follows every
+                    // retirement of this relabel, so all blocks agree)
+                    const unsigned long long live = (unsigned long long)g.n - vload(&ctl->retired_nodes);
+                    budget = (unsigned long long)((double)p.budget * ((double)live / (double)g.n)) + 1ull;
+                }
                 if (p.relabel_rounds && r >= p.relabel_rounds) break;
-                if (p.budget && visits > p.budget) break;
+                if (budget && visits > budget) break;
             }
             if (!ok) break;
             if (lead) {
-                for (int k = 0; k < 3; ++k) { ctl->act_cnt[k] = 0u; ctl->bfs_cnt[k] = 0u; }
+                for (int k = 0; k < 3; ++k) {
+                    ctl->act_cnt[k] = 0u;
+                    ctl->bfs_cnt[k] = 0u;
+                    ctl->lab_cnt[k] = 0u;
+                    ctl->bu_cnt[k] = 0u;
+                }
+                // the reached set of this relabel: the next one's candidates
+                ctl->cand_cnt = ctl->cand_build;
+                ctl->bu_cnt[0] = ctl->cand_build;
+                ctl->cand_build = 0u;
             }
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
             lap(2);
@@ -807,6 +973,24 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
         }
     }
     reduce_work(ctl, w, bfs_visits, s_red);
+}
+
+// First graph of every sweep chunk: the largest k with off[k] <= the chunk's
+// first node.
+__global__ void __launch_bounds__(DTPB) k_chunk_seg(uint32_t nchunks, uint32_t nseg,
+                                                    const uint32_t* __restrict__ off,
+                                                    uint32_t* __restrict__ chunk_seg)
+{
+    for (uint32_t c = blockIdx.x * DTPB + threadIdx.x; c < nchunks; c += gridDim.x * DTPB) {
+        const uint32_t v0 = c * SWEEP_CHUNK;
+        uint32_t lo = 0, hi = nseg;
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(off + mid) <= v0) lo = mid;
+            else hi = mid;
+        }
+        chunk_seg[c] = lo;
+    }
 }
 
 __global__ void __launch_bounds__(DTPB) k_prepare_raw(uint32_t n, const int4* __restrict__ nbr,
@@ -898,6 +1082,8 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
         r.engine = o->engine;
         if (o->chain_hops > 0) r.chain_hops = o->chain_hops;
         if (o->chain_max_active > 0) r.chain_max_active = o->chain_max_active;
+        r.bfs_bottom_up = o->bfs_bottom_up;
+        if (o->bfs_bottom_up_ratio > 0) r.bfs_bottom_up_ratio = o->bfs_bottom_up_ratio;
     }
     // clamps of gpu_push_relabel_fast.cu:421-424 and :476-480
     if (ls < 1) ls = 1;
@@ -1020,12 +1206,15 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     out.bfs_ms = (double)(hc.bfs_ns + hc.sweep_ns) * 1e-6;
     out.discharge_ms = (double)hc.discharge_ns * 1e-6;
     out.sweep_ms = (double)hc.sweep_ns * 1e-6;
+    out.graphs_retired = hc.segs_retired;
+    out.bottom_up_steps = hc.bu_steps;
     out.solve_s = std::chrono::duration<double>(Clock::now() - t0).count();
 }
 
 void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const uint8_t* d_rev,
                         const uint32_t* d_pair, int32_t* d_term, SolveWorkspace& w,
-                        const SolveOptions& opt, cudaStream_t s, SolveResult& out)
+                        const SolveOptions& opt, cudaStream_t s, SolveResult& out,
+                        const Segments* segments)
 {
     using Clock = std::chrono::steady_clock;
     out = SolveResult{};
@@ -1057,7 +1246,42 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
     g.local_steps = opt.local_steps;
 
     if (use_persistent_engine(opt)) {
+        if (segments && segments->nseg > 1u && segments->d_off) {
+            const uint32_t nseg = segments->nseg;
+            const uint32_t nchunks = (n + SWEEP_CHUNK - 1u) / SWEEP_CHUNK;
+            if (w.chunk_seg.n < nchunks) w.chunk_seg = DevBuf<uint32_t>(nchunks, s);
+            if (w.seg_live.n < nseg) {
+                w.seg_live = DevBuf<uint32_t>(nseg, s);
+                w.seg_act = DevBuf<uint32_t>(nseg, s);
+            }
+            GPUPR_CUDA(cudaMemsetAsync(w.seg_live.p, 0x01, (size_t)nseg * 4u, s));   // all live
+            GPUPR_CUDA(cudaMemsetAsync(w.seg_act.p, 0, (size_t)nseg * 4u, s));
+            const unsigned cg = (unsigned)std::min<uint32_t>((nchunks + DTPB - 1u) / DTPB,
+                                                             (uint32_t)sm_count() * 8u);
+            k_chunk_seg<<<cg, DTPB, 0, s>>>(nchunks, nseg, segments->d_off, w.chunk_seg.p);
+            GPUPR_CUDA(cudaGetLastError());
+            out.launches += 1;
+            g.nseg = nseg;
+            g.seg_off = segments->d_off;
+            g.chunk_seg = w.chunk_seg.p;
+            g.seg_live = w.seg_live.p;
+            g.seg_act = w.seg_act.p;
+            out.workspace_bytes = w.bytes();
+        }
+        if (opt.bfs_bottom_up) {
+            if (w.cand0.n < n) {
+                w.cand0 = DevBuf<uint32_t>(n, s);
+                w.cand1 = DevBuf<uint32_t>(n, s);
+            }
+            g.cand[0] = w.cand0.p;
+            g.cand[1] = w.cand1.p;
+            g.bottom_up = 1;
+            g.bu_ratio = (float)(opt.bfs_bottom_up_ratio > 0 ? opt.bfs_bottom_up_ratio : 1.0);
+            out.workspace_bytes = w.bytes();
+        }
+        const uint64_t pre = out.launches;
         solve_persistent(g, opt, s, out);
+        out.launches += pre;
         return;
     }
     out.engine = 1;

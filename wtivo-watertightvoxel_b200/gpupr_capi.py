@@ -37,6 +37,8 @@ STATS_FIELDS = [
     ("bfs_launches", ctypes.c_uint64), ("engine", ctypes.c_int64),
     ("solve_blocks_per_sm", ctypes.c_int64), ("relabel_work_factor", ctypes.c_double),
     ("chain_hops", ctypes.c_int64), ("chain_max_active", ctypes.c_int64),
+    ("sweep_ms", ctypes.c_double), ("graphs_retired", ctypes.c_uint64),
+    ("bottom_up_steps", ctypes.c_uint64),
 ]
 
 
@@ -55,6 +57,7 @@ class SolveOptions(ctypes.Structure):
         ("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
         ("work_relabel_factor", ctypes.c_double), ("engine", ctypes.c_int32),
         ("chain_hops", ctypes.c_int32), ("chain_max_active", ctypes.c_int32),
+        ("bfs_bottom_up", ctypes.c_int32), ("bfs_bottom_up_ratio", ctypes.c_double),
     ]
 
 
