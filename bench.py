@@ -913,12 +913,15 @@ def run_batch(args, local):
 
 
 def run_serve(args):
-    """Config 5: Poisson arrivals at 20 req/s, tets log-uniform 100k..20M,
-    160 GiB admission budget.  The same arrival trace goes through the
-    continuous-batching server, through the same server one request at a time
-    (max_batch 1: FIFO, uploads still overlapping the previous cut), and is
-    replayed against one-at-a-time service times measured alone (host arrays
-    copied in, cut, labels copied out: the naive FIFO)."""
+    """Config 5: Poisson arrivals, tets log-uniform 100k..20M (a pool of 12
+    seeded graphs), 160 GiB admission budget, host arrays in and out.  At 20
+    req/s (the config's rate) and at 100 req/s (a load where requests queue),
+    the same arrival trace goes through the server with its two lanes (small
+    requests below 2M tets solve beside large ones), through one lane
+    (continuous batching, one solve at a time), and through one lane one
+    request at a time (max_batch 1); the 20 req/s trace is also replayed
+    against one-at-a-time service times measured alone (the naive FIFO).
+    Latency p50/p99 overall and p99 per size bucket."""
     import threading
 
     import torch
@@ -929,9 +932,7 @@ def run_serve(args):
     rng = np.random.default_rng(args.seed + 5)
     pool_sizes = np.exp(rng.uniform(np.log(1e5), np.log(2e7), size=12)).astype(np.int64)
     pool = [synth.config3_graph(i, int(n), args.seed + 5) for i, n in enumerate(pool_sizes)]
-    n_req = int(20 * args.serve_seconds)
-    arrivals = np.cumsum(rng.exponential(1 / 20.0, size=n_req))
-    picks = rng.integers(len(pool), size=n_req)
+    split = 2_000_000
 
     # service time of each pool graph alone: host topology -> device, cut, labels out
     service = []
@@ -947,11 +948,17 @@ def run_serve(args):
             del tt, nn
         service.append(dt)
 
-    def trace(max_batch):
+    def make_trace(rate, seconds):
+        r = np.random.default_rng(args.seed + 7 + int(rate))
+        n = int(rate * seconds)
+        return np.cumsum(r.exponential(1 / rate, size=n)), r.integers(len(pool), size=n)
+
+    def run(arrivals, picks, max_batch, split_tets):
+        n_req = len(arrivals)
         results = {}
-        with gpupr_capi.Server(hbm_budget_bytes=160 << 30, max_batch=max_batch) as sv:
-            g0 = pool[0]
-            sv.wait(sv.submit(g0["vertices"], g0["tets"], g0["neighbors"], g0["labels"]))
+        with gpupr_capi.Server(hbm_budget_bytes=160 << 30, max_batch=max_batch, split_tets=split_tets) as sv:
+            for g0 in (pool[0], pool[int(np.argmax(pool_sizes))]):
+                sv.wait(sv.submit(g0["vertices"], g0["tets"], g0["neighbors"], g0["labels"]))
             ids = []
             t_start = time.perf_counter()
 
@@ -976,30 +983,40 @@ def run_serve(args):
             wall = time.perf_counter() - t_start
         lat = np.array([results[k]["latency_ms"] for k in range(n_req)])
         bs = np.array([results[k]["batch_size"] for k in range(n_req)])
-        up = np.array([results[k]["upload_ms"] for k in range(n_req)])
-        sv_ms = np.array([results[k]["solve_ms"] for k in range(n_req)])
+        small = np.array([len(pool[picks[k]]["labels"]) < split for k in range(n_req)])
+
+        def p99(m):
+            return round(float(np.percentile(lat[m], 99)), 2) if m.any() else None
+
         return {"p50_ms": round(float(np.percentile(lat, 50)), 2),
                 "p99_ms": round(float(np.percentile(lat, 99)), 2),
+                "p99_small_ms": p99(small), "p99_large_ms": p99(~small),
+                "p50_small_ms": round(float(np.percentile(lat[small], 50)), 2) if small.any() else None,
                 "cuts_per_s": round(n_req / wall, 2), "mean_batch": round(float(bs.mean()), 2),
-                "max_batch": int(bs.max()), "mean_upload_ms": round(float(up.mean()), 2),
-                "mean_solve_ms": round(float(sv_ms.mean()), 2)}
+                "max_batch": int(bs.max())}
 
-    batched = trace(0)
-    one_at_a_time = trace(1)
-    free_at, seq_lat = 0.0, []
-    for k in range(n_req):
-        start = max(arrivals[k], free_at)
-        free_at = start + service[picks[k]]
-        seq_lat.append(1e3 * (free_at - arrivals[k]))
-    seq_lat = np.array(seq_lat)
-    return {"config": "Poisson 20 req/s for %.0f s, tets log-uniform 100k..20M (pool of 12 "
-                      "seeded graphs), 160 GiB budget, host arrays in and out" % args.serve_seconds,
-            "requests": n_req, "mean_tets_per_request": int(np.mean([len(pool[p]["labels"]) for p in picks])),
-            **batched,
-            "server_max_batch_1": one_at_a_time,
-            "naive_fifo": {"p50_ms": round(float(np.percentile(seq_lat, 50)), 2),
-                           "p99_ms": round(float(np.percentile(seq_lat, 99)), 2),
-                           "mean_service_ms": round(1e3 * float(np.mean([service[p] for p in picks])), 2)}}
+    out = {"config": "Poisson arrivals, tets log-uniform 100k..20M (pool of 12 seeded graphs), "
+                     "160 GiB budget, host arrays in and out; small = under 2M tets",
+           "lane_split_tets": split}
+    for rate, seconds in ((20.0, args.serve_seconds), (100.0, args.serve_seconds / 2)):
+        arrivals, picks = make_trace(rate, seconds)
+        leg = {"requests": len(arrivals),
+               "mean_tets_per_request": int(np.mean([len(pool[p]["labels"]) for p in picks])),
+               "two_lanes": run(arrivals, picks, 0, None),
+               "one_lane": run(arrivals, picks, 0, 0),
+               "one_lane_max_batch_1": run(arrivals, picks, 1, 0)}
+        if rate == 20.0:
+            free_at, seq_lat = 0.0, []
+            for k in range(len(arrivals)):
+                start = max(arrivals[k], free_at)
+                free_at = start + service[picks[k]]
+                seq_lat.append(1e3 * (free_at - arrivals[k]))
+            seq_lat = np.array(seq_lat)
+            leg["naive_fifo"] = {"p50_ms": round(float(np.percentile(seq_lat, 50)), 2),
+                                 "p99_ms": round(float(np.percentile(seq_lat, 99)), 2),
+                                 "mean_service_ms": round(1e3 * float(np.mean([service[p] for p in picks])), 2)}
+        out[f"rate_{int(rate)}"] = leg
+    return out
 
 
 def run_reference(args, world, rank, local):

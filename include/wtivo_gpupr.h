@@ -204,11 +204,12 @@ gpupr_status gpupr_graph_cut_batch(uint32_t n_graphs, const uint64_t* tet_offset
 
 /*
  * Serving loop (continuous batching).  No counterpart in the reference.
- * A server owns two threads on the device current at creation: a stager that
- * admits requests in arrival order while their estimated device footprint
- * fits hbm_budget_bytes (0 = 160 GiB) next to the batch being solved and
- * uploads them as one packed batch, and a solver that cuts each staged batch
- * in one solve.  Requests that arrive while a batch runs join the next one.
+ * A server owns, per lane, two threads on the device current at creation: a
+ * stager that admits the lane's requests in arrival order while their
+ * estimated device footprint fits hbm_budget_bytes (0 = 160 GiB) next to
+ * every batch staged or being solved and uploads them as one packed batch,
+ * and a solver that cuts each staged batch in one solve.  Requests that
+ * arrive while a batch runs join the lane's next one.
  * A request is one cell graph in HOST arrays with graph_cut_fast's layout;
  * the server BORROWS them (no copy): vertices, tets, neighbors and labels
  * must stay valid and unchanged, and out_labels (n_tets bytes) writable,
@@ -228,12 +229,25 @@ typedef struct {
     double upload_ms;         /* the batch's host -> device copies */
     double solve_ms;          /* the batch's cut, labels copied out */
     double latency_ms;        /* submit -> result ready */
+    int32_t lane;             /* 0 small-request lane, 1 large-request lane */
+    int32_t reserved;
 } gpupr_request_result;
 
-/* max_batch: most requests per batch (0 = no limit; 1 = one request at a
- * time, uploads still overlapping the previous cut). */
+/* max_batch: most requests per batch and lane (0 = no limit; 1 = one request
+ * at a time per lane, uploads still overlapping the previous cut).
+ * gpupr_server_create splits requests at 2,000,000 tets into two lanes whose
+ * solves run at the same time: requests below the split go to the small lane
+ * (its persistent grid capped at 1 resident block per SM), the rest to the
+ * large lane (capped at the solver kernel's occupancy limit minus one), so
+ * both lanes' grids are resident together and a small request never waits
+ * for a large one's solve.  The HBM budget covers both lanes.
+ * gpupr_server_create_lanes takes the split; split_tets = 0 gives one lane
+ * (every solve on the whole GPU, one at a time). */
 gpupr_status gpupr_server_create(uint64_t hbm_budget_bytes, uint32_t max_batch,
                                  const gpupr_solve_options* options, gpupr_server** server);
+gpupr_status gpupr_server_create_lanes(uint64_t hbm_budget_bytes, uint32_t max_batch,
+                                       const gpupr_solve_options* options, uint64_t split_tets,
+                                       gpupr_server** server);
 gpupr_status gpupr_server_submit(gpupr_server* server, const double* vertices,
                                  uint64_t n_vertices, const int32_t* tets,
                                  const int32_t* neighbors, const uint8_t* labels,

@@ -103,3 +103,28 @@ def test_bad_request_does_not_fail_its_batch(built):
             lab, st = want[gi]
             assert res["status"] == 0 and np.array_equal(out, lab)
             assert res["adjusted_flow"] == st["adjusted_flow"]
+
+
+@pytest.mark.parametrize("split", [0, 100_000])
+def test_lanes_give_exact_cuts(built, split):
+    """Requests split by size into two lanes whose solves overlap (or one lane
+    with split 0): every result equals its cut alone, and each request took
+    the lane its size selects."""
+    import gpupr_capi
+
+    big = cached_graph("lattice", 3, 300_000)
+    pool = _pool() + [big]
+    want = [orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0) for g in pool]
+    with gpupr_capi.Server(split_tets=split) as sv:
+        ids = []
+        for rep in range(3):
+            for gi in (4, 0, 1, 2, 3):
+                g = pool[gi]
+                ids.append((gi, sv.submit(g["vertices"], g["tets"], g["neighbors"], g["labels"])))
+        for gi, rid in ids:
+            out, res = sv.wait(rid, timeout_s=120)
+            lab, st = want[gi]
+            assert res["status"] == 0 and np.array_equal(out, lab), gi
+            assert res["adjusted_flow"] == st["adjusted_flow"]
+            n = len(pool[gi]["tets"])
+            assert res["lane"] == (1 if split and n >= split else 0), (gi, n)

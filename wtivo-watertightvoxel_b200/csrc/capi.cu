@@ -331,7 +331,8 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
                          const double* vertices, int v_dev, const int32_t* d_tets_l,
                          const int32_t* d_nbrs_l, const uint8_t* labels, int l_dev, double fill_T,
                          const gpupr_solve_options* options, uint8_t* out, int out_dev,
-                         cudaStream_t s, gpupr_batch_item* items, gpupr_cut_stats* st)
+                         cudaStream_t s, gpupr_batch_item* items, gpupr_cut_stats* st,
+                         int max_blocks_per_sm)
 {
     const auto all0 = std::chrono::steady_clock::now();
     if (!st || !items || !toff || !voff) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL batch argument"};
@@ -426,6 +427,7 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     segs.nseg = G;
     segs.d_off = d_soff.p;
 
+    opt.max_blocks_per_sm = max_blocks_per_sm;
     SolveWorkspace w;
     SolveResult sr;
     solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr, &segs);

@@ -260,6 +260,8 @@ struct SolveOptions {
     int chain_max_active = 0;      // persistent engine: 0 = default
     int bfs_bottom_up = 0;         // persistent engine: direction-optimizing relabels
     double bfs_bottom_up_ratio = 1.0;
+    int max_blocks_per_sm = 0;     // persistent engine: cap on the grid (0 = none); the
+                                   // server's lanes use it so their solves fit side by side
 };
 
 SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw,
@@ -370,12 +372,18 @@ void compute_reverse_slots_noalloc(uint32_t n, const int4* d_nbr, const uint32_t
                                    uint8_t* d_rev, uint32_t* d_pair, int32_t* d_err,
                                    cudaStream_t s);
 
-// Batched graph cut (capi.cu), used by the C ABI and the serving loop.
+// Batched graph cut (capi.cu), used by the C ABI and the serving loop;
+// max_blocks_per_sm caps the persistent solve's grid (0 = no cap).
 void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
                          const double* vertices, int v_dev, const int32_t* d_tets_l,
                          const int32_t* d_nbrs_l, const uint8_t* labels, int l_dev, double fill_T,
                          const gpupr_solve_options* options, uint8_t* out, int out_dev,
-                         cudaStream_t s, gpupr_batch_item* items, gpupr_cut_stats* st);
+                         cudaStream_t s, gpupr_batch_item* items, gpupr_cut_stats* st,
+                         int max_blocks_per_sm = 0);
+
+// Resident blocks per SM of the persistent solver kernel on the current
+// device (its occupancy limit).
+int persistent_blocks_per_sm();
 
 // Bounded wait self test kernel driver.
 gpupr_status bounded_wait_selftest(uint32_t limit_us, cudaStream_t s);

@@ -1097,6 +1097,13 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
     return r;
 }
 
+int persistent_blocks_per_sm()
+{
+    int bps = 0;
+    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent, DTPB, 0));
+    return bps;
+}
+
 bool use_persistent_engine(const SolveOptions& opt)
 {
     if (opt.engine == 1) return false;
@@ -1130,7 +1137,8 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
                      : g.n < 6000000u       ? 2
                      : g.n < 40000000u      ? 3
                                             : 4;
-    const int used = want < bps ? want : bps;
+    int used = want < bps ? want : bps;
+    if (opt.max_blocks_per_sm > 0 && used > opt.max_blocks_per_sm) used = opt.max_blocks_per_sm;
     const unsigned grid = (unsigned)(sm_count() * used);
     PersistParams p{};
     p.max_rounds = opt.max_rounds;

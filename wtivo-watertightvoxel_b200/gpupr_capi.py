@@ -71,7 +71,8 @@ class RequestResult(ctypes.Structure):
                 ("adjusted_flow", ctypes.c_int64), ("raw_flow", ctypes.c_int64),
                 ("n_tets", ctypes.c_uint64), ("free_n", ctypes.c_uint64),
                 ("queue_ms", ctypes.c_double), ("upload_ms", ctypes.c_double),
-                ("solve_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+                ("solve_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("lane", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class GpuprError(RuntimeError):
@@ -125,6 +126,8 @@ def lib():
         L.gpupr_graph_cut_batch.argtypes = [ctypes.c_uint32, p, p, p, ctypes.c_int, p, p, p,
                                             ctypes.c_int, f64, p, p, ctypes.c_int, p, p, p]
         L.gpupr_server_create.argtypes = [ctypes.c_uint64, ctypes.c_uint32, p, ctypes.POINTER(p)]
+        L.gpupr_server_create_lanes.argtypes = [ctypes.c_uint64, ctypes.c_uint32, p, ctypes.c_uint64,
+                                                ctypes.POINTER(p)]
         L.gpupr_server_submit.argtypes = [p, p, ctypes.c_uint64, p, p, p, ctypes.c_uint64, f64,
                                           p, ctypes.POINTER(ctypes.c_uint64)]
         L.gpupr_server_wait.argtypes = [p, ctypes.c_uint64, f64, p]
@@ -259,17 +262,21 @@ def graph_cut_batch(toff, voff, vertices, tets, nbrs, labels, fill_T, opts=None,
 
 class Server:
     """Continuous-batching cut server (gpupr_server_*): submit() host graphs
-    at any time, wait() for each result."""
+    at any time, wait() for each result.  split_tets=None: the library's
+    default two lanes (split at 2M tets); 0: one lane; else the split."""
 
-    def __init__(self, hbm_budget_bytes=0, opts=None, max_batch=0):
+    def __init__(self, hbm_budget_bytes=0, opts=None, max_batch=0, split_tets=None):
         import torch
 
         torch.cuda.init()
         lib()
         self._h = ctypes.c_void_p()
-        check(_lib.gpupr_server_create(int(hbm_budget_bytes), int(max_batch),
-                                       ctypes.byref(opts) if opts is not None else None,
-                                       ctypes.byref(self._h)))
+        o = ctypes.byref(opts) if opts is not None else None
+        if split_tets is None:
+            check(_lib.gpupr_server_create(int(hbm_budget_bytes), int(max_batch), o, ctypes.byref(self._h)))
+        else:
+            check(_lib.gpupr_server_create_lanes(int(hbm_budget_bytes), int(max_batch), o,
+                                                 int(split_tets), ctypes.byref(self._h)))
         self._held = {}
 
     def submit(self, vertices, tets, nbrs, labels, fill_T=10.0):
