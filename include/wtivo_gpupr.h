@@ -188,10 +188,14 @@ typedef struct {
  * host arrays of n_graphs+1 entries starting at 0.  out_labels is the
  * concatenation of every graph's graph_cut_fast labels; items[g] receives
  * each graph's flows.  One fill_T and one set of options for the batch.
- * Unless options set chain_hops, chain_max_active or blocks_per_sm, a batch
- * of at least 16 graphs averaging under 1.5M tets solves with 8 chained
- * hops in rounds of up to 131072 active nodes on 3 blocks per SM (the
- * setting that suits small graphs; the union's own size would pick another).
+ * The union is solved as segments: each graph retires once a global relabel
+ * finds no active node in it (its labels are then final and later relabels
+ * skip it).  Unless options set chain_hops, chain_max_active, blocks_per_sm or
+ * work_relabel_factor, the batch takes the batch tuning table's entry for its
+ * size bucket (gpupr_autotune_batch); without one, a batch of at least 16
+ * graphs averaging under 1.5M tets solves with 8 chained hops in rounds of up
+ * to 131072 active nodes on 3 blocks per SM (the setting that suits small
+ * graphs; the union's own size would pick another).
  */
 gpupr_status gpupr_graph_cut_batch(uint32_t n_graphs, const uint64_t* tet_offsets,
                                    const uint64_t* vertex_offsets, const double* vertices,
@@ -475,6 +479,25 @@ gpupr_status gpupr_autotune(const double* vertices, uint64_t n_vertices, int ver
                             void* stream);
 gpupr_status gpupr_tune_table(gpupr_tune_entry* entries, uint32_t capacity, uint32_t* count);
 gpupr_status gpupr_tune_table_set(const gpupr_tune_entry* entries, uint32_t count);
+
+/*
+ * Batch autotuner (no counterpart in the reference): the same two stages as
+ * gpupr_autotune on one batch (arguments as gpupr_graph_cut_batch), timing
+ * the segmented solve of its union against the batch rule (the one
+ * gpupr_graph_cut_batch applies when no entry exists).  The chosen setting is
+ * kept in a separate per-process table keyed by the batch's size bucket: the
+ * size class of its free nodes per graph (in [2^k, 2^(k+1))).  Later batches
+ * whose options leave blocks_per_sm, work_relabel_factor, chain_hops and
+ * chain_max_active at 0 take their bucket's entry.
+ */
+gpupr_status gpupr_autotune_batch(uint32_t n_graphs, const uint64_t* tet_offsets,
+                                  const uint64_t* vertex_offsets, const double* vertices,
+                                  int vertices_on_device, const int32_t* d_tets,
+                                  const int32_t* d_neighbors, const uint8_t* labels,
+                                  int labels_on_device, double fill_T, int32_t local_steps,
+                                  int32_t reps, gpupr_tune_entry* chosen, void* stream);
+gpupr_status gpupr_batch_tune_table(gpupr_tune_entry* entries, uint32_t capacity, uint32_t* count);
+gpupr_status gpupr_batch_tune_table_set(const gpupr_tune_entry* entries, uint32_t count);
 
 /* Release device memory cached between calls (pool + scratch). */
 gpupr_status gpupr_release_cached_memory(void);

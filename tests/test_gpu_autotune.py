@@ -5,8 +5,10 @@ from __future__ import annotations
 
 import numpy as np
 import pytest
+import torch
 
 from conftest import cached_graph, to_cuda
+from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
 
@@ -36,3 +38,28 @@ def test_autotune_then_cut(built):
     gpupr_capi.set_tune_table([])
     _, st3 = gpupr_capi.graph_cut(g["vertices"], tets, nbrs, g["labels"], g["fill_T"])
     assert st3["solve_blocks_per_sm"] == st0["solve_blocks_per_sm"]
+
+
+def test_batch_autotune_keeps_cuts_and_fills_its_bucket(built):
+    """The batch tuner times the segmented solve of one batch and keeps an
+    entry for the batch's size bucket; a batch cut with that entry gives every
+    graph its own cut."""
+    import gpupr_capi
+
+    graphs = [cached_graph("proxy", 0, 20_000), cached_graph("box", 4, 60_000),
+              cached_graph("torus", 5, 60_000), cached_graph("lattice", 2, 80_000)]
+    toff, voff, V, T, Nb, L = gpupr_capi.pack_batch(graphs)
+    t, n = torch.from_numpy(T).cuda(), torch.from_numpy(Nb).cuda()
+    old = gpupr_capi.batch_tune_table()
+    try:
+        e = gpupr_capi.autotune_batch(toff, voff, V, t, n, L, 10.0, reps=1)
+        assert e["blocks_per_sm"] >= 1 and e["solve_ms"] > 0 and e["solve_ms"] <= e["default_ms"] * 1.5
+        assert any(x["size_class"] == e["size_class"] for x in gpupr_capi.batch_tune_table())
+        out, items, st = gpupr_capi.graph_cut_batch(toff, voff, V, t, n, L, 10.0)
+        assert st["solve_blocks_per_sm"] == e["blocks_per_sm"] and st["chain_hops"] == e["chain_hops"]
+        for k, g in enumerate(graphs):
+            lab, ost = orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0)
+            assert np.array_equal(out[int(toff[k]):int(toff[k + 1])], lab), k
+            assert items[k]["adjusted_flow"] == ost["adjusted_flow"]
+    finally:
+        gpupr_capi.set_batch_tune_table(old)

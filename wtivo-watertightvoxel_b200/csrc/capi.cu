@@ -222,9 +222,86 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
     st->native_total_seconds = seconds_since(all0);
 }
 
-// gpupr_autotune: one build, then timed solves of the same reduced graph
-// (residuals and terminals restored before each) under every candidate pair,
-// interleaved so slow drifts of the clock hit every pair alike.
+// Tuning of the persistent engine's free choices on one reduced graph (or a
+// batch's segmented union): timed solves with the residuals and terminals
+// restored before each, every candidate `reps` times, interleaved so slow
+// drifts of the clock hit every candidate alike.  Stage 1: resident blocks per
+// SM x relabel work factor with the base chaining; stage 2: chaining with the
+// best pair.  Both stages also time `base` itself (the built-in rule), and the
+// entry never replaces the rule by a setting that was not faster.  A
+// candidate's zero fields take base's values.
+struct TuneCand {
+    int bps;
+    double wf;
+    int hops, cmax;
+    std::vector<double> ms;
+    SolveResult last;   // settings the solve actually used
+};
+
+double median_of(std::vector<double> v)
+{
+    std::sort(v.begin(), v.end());
+    return v.size() % 2 ? v[v.size() / 2] : 0.5 * (v[v.size() / 2 - 1] + v[v.size() / 2]);
+}
+
+TuneEntry two_stage_tune(ReducedGraph& g, const Segments* segs, const gpupr_solve_options& base,
+                         int32_t local_steps, int32_t reps, cudaStream_t s)
+{
+    DevBuf<uint32_t> res0(4u * (size_t)g.n, s);
+    DevBuf<int32_t> term0(g.n, s);
+    GPUPR_CUDA(cudaMemcpyAsync(res0.p, g.res.p, 16u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+    GPUPR_CUDA(cudaMemcpyAsync(term0.p, g.term.p, 4u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+    SolveWorkspace w;
+    auto run = [&](std::vector<TuneCand>& cands) {
+        for (int r = 0; r < reps; ++r)
+            for (TuneCand& c : cands) {
+                GPUPR_CUDA(cudaMemcpyAsync(g.res.p, res0.p, 16u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+                GPUPR_CUDA(cudaMemcpyAsync(g.term.p, term0.p, 4u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
+                gpupr_solve_options o = base;
+                o.local_steps = local_steps;
+                o.engine = 2;
+                if (c.bps) o.blocks_per_sm = c.bps;
+                if (c.wf > 0) o.work_relabel_factor = c.wf;
+                if (c.hops) o.chain_hops = c.hops;
+                if (c.cmax) o.chain_max_active = c.cmax;
+                SolveOptions opt = resolve_options(&o, local_steps, 1024, 2000000ull);
+                SolveResult sr;
+                solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr, segs);
+                c.ms.push_back(sr.solve_device_ms);
+                c.last = sr;
+            }
+    };
+    std::vector<TuneCand> c1;
+    c1.push_back({0, 0.0, 0, 0, {}, {}});
+    for (int bp : {1, 2, 3, 4})
+        for (double f : {0.5, 1.0, 2.0}) c1.push_back({bp, f, 0, 0, {}, {}});
+    run(c1);
+    size_t bi = 1;
+    for (size_t i = 2; i < c1.size(); ++i)
+        if (median_of(c1[i].ms) < median_of(c1[bi].ms)) bi = i;
+    std::vector<TuneCand> c2;
+    c2.push_back({0, 0.0, 0, 0, {}, {}});
+    for (auto hc : {std::pair<int, int>{1, 1}, {4, 4096}, {4, 32768}, {8, 131072}})
+        c2.push_back({c1[bi].bps, c1[bi].wf, hc.first, hc.second, {}, {}});
+    run(c2);
+    size_t bj = 0;
+    for (size_t i = 1; i < c2.size(); ++i)
+        if (median_of(c2[i].ms) < median_of(c2[bj].ms)) bj = i;
+    const TuneCand& win = c2[bj];
+    TuneEntry best;
+    best.blocks_per_sm = win.last.blocks_per_sm;
+    best.work_factor = win.last.work_factor;
+    best.chain_hops = win.last.chain_hops;
+    best.chain_max_active = win.last.chain_max_active;
+    best.solve_ms = median_of(win.ms);
+    std::vector<double> dflt = c1[0].ms;
+    dflt.insert(dflt.end(), c2[0].ms.begin(), c2[0].ms.end());
+    best.default_ms = median_of(dflt);
+    return best;
+}
+
+// gpupr_autotune: one build, then the two-stage tuning of its solve; the
+// entry is kept for the graph's size class.
 TuneEntry run_autotune(const double* vertices, uint64_t nv, int v_dev, const int32_t* d_tets,
                        const int32_t* d_nbrs, uint64_t N, const uint8_t* labels, int l_dev,
                        double fill_T, int32_t local_steps, int32_t reps, cudaStream_t s)
@@ -247,41 +324,6 @@ TuneEntry run_autotune(const double* vertices, uint64_t nv, int v_dev, const int
     uint64_t launches = 0;
     build_reduced_graph(in, g, info, s, &launches);
     if (info.free_n == 0) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "autotune: the cut has no free tet"};
-    DevBuf<uint32_t> res0(4u * (size_t)g.n, s);
-    DevBuf<int32_t> term0(g.n, s);
-    GPUPR_CUDA(cudaMemcpyAsync(res0.p, g.res.p, 16u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
-    GPUPR_CUDA(cudaMemcpyAsync(term0.p, g.term.p, 4u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
-    struct Cand {
-        int bps;
-        double wf;
-        int hops, cmax;
-        std::vector<double> ms;
-        SolveResult last;   // settings the solve actually used
-    };
-    SolveWorkspace w;
-    auto run = [&](std::vector<Cand>& cands) {
-        for (int r = 0; r < reps; ++r)
-            for (Cand& c : cands) {
-                GPUPR_CUDA(cudaMemcpyAsync(g.res.p, res0.p, 16u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
-                GPUPR_CUDA(cudaMemcpyAsync(g.term.p, term0.p, 4u * (size_t)g.n, cudaMemcpyDeviceToDevice, s));
-                gpupr_solve_options o{};
-                o.local_steps = local_steps;
-                o.engine = 2;
-                o.blocks_per_sm = c.bps;
-                o.work_relabel_factor = c.wf;
-                o.chain_hops = c.hops;
-                o.chain_max_active = c.cmax;
-                SolveOptions opt = resolve_options(&o, local_steps, 1024, 2000000ull);
-                SolveResult sr;
-                solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr);
-                c.ms.push_back(sr.solve_device_ms);
-                c.last = sr;
-            }
-    };
-    auto median = [](std::vector<double> v) {
-        std::sort(v.begin(), v.end());
-        return v.size() % 2 ? v[v.size() / 2] : 0.5 * (v[v.size() / 2 - 1] + v[v.size() / 2]);
-    };
     // the built-in rule (an empty table: the rule, not an older entry)
     TuneEntry old;
     if (tune_lookup(g.n, &old)) {
@@ -291,38 +333,109 @@ TuneEntry run_autotune(const double* vertices, uint64_t nv, int v_dev, const int
                    keep.end());
         tune_replace(keep);
     }
-    // stage 1: grid x relabel schedule, default chaining
-    std::vector<Cand> c1;
-    c1.push_back({0, 0.0, 0, 0, {}, {}});
-    for (int b : {1, 2, 3, 4})
-        for (double f : {0.5, 1.0, 2.0}) c1.push_back({b, f, 0, 0, {}, {}});
-    run(c1);
-    size_t bi = 1;
-    for (size_t i = 2; i < c1.size(); ++i)
-        if (median(c1[i].ms) < median(c1[bi].ms)) bi = i;
-    // stage 2: chaining with the best pair, against the built-in rule again:
-    // the entry never replaces the rule by a setting that was not faster
-    std::vector<Cand> c2;
-    c2.push_back({0, 0.0, 0, 0, {}, {}});
-    for (auto hc : {std::pair<int, int>{1, 1}, {4, 4096}, {4, 32768}, {8, 131072}})
-        c2.push_back({c1[bi].bps, c1[bi].wf, hc.first, hc.second, {}, {}});
-    run(c2);
-    size_t bj = 0;
-    for (size_t i = 1; i < c2.size(); ++i)
-        if (median(c2[i].ms) < median(c2[bj].ms)) bj = i;
-    const Cand& win = c2[bj];
-    TuneEntry best;
+    gpupr_solve_options base{};
+    TuneEntry best = two_stage_tune(g, nullptr, base, local_steps, reps, s);
     best.size_class = size_class(g.n);
-    best.blocks_per_sm = win.bps ? win.bps : win.last.blocks_per_sm;
-    best.work_factor = win.wf > 0 ? win.wf : win.last.work_factor;
-    best.chain_hops = win.hops ? win.hops : win.last.chain_hops;
-    best.chain_max_active = win.cmax ? win.cmax : win.last.chain_max_active;
-    best.solve_ms = median(win.ms);
-    std::vector<double> dflt = c1[0].ms;
-    dflt.insert(dflt.end(), c2[0].ms.begin(), c2[0].ms.end());
-    best.default_ms = median(dflt);
     tune_store(best);
     return best;
+}
+
+// A batch packed, its union's reduced graph built, and each graph's range of
+// reduced ids (the segments of the solve and of the per-graph flows).
+struct PreparedBatch {
+    DevBuf<uint8_t> dlab;
+    DevBuf<double> dver;
+    const uint8_t* d_labels = nullptr;
+    DevBuf<unsigned long long> d_toff, d_voff, d_foff;
+    DevBuf<uint32_t> d_soff;
+    DevBuf<int32_t> gt, gn;
+    ReducedGraph g;
+    BuildInfo info;
+    std::vector<unsigned long long> hc;   // free nodes per graph
+    Segments segs;
+};
+
+// Checks the offsets and prepares the batch; stops after the build when no
+// tet is free (pb.info.free_n == 0).
+void prepare_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff, const double* vertices,
+                   int v_dev, const int32_t* d_tets_l, const int32_t* d_nbrs_l, const uint8_t* labels,
+                   int l_dev, double fill_T, cudaStream_t s, PreparedBatch& pb, uint64_t* launches)
+{
+    if (toff[0] != 0 || voff[0] != 0) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "batch offsets must start at 0"};
+    for (uint32_t k = 0; k < G; ++k)
+        if (toff[k + 1] < toff[k] || voff[k + 1] < voff[k])
+            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "batch offsets must be non-decreasing"};
+    const uint64_t N = toff[G], nv = voff[G];
+    if (N > 0x7FFFFFFEull) throw Error{GPUPR_ERR_TOO_MANY_TETS, "batch exceeds 2^31-1 tets"};
+    if (!d_tets_l || !d_nbrs_l || !labels || (!vertices && nv))
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL batch array"};
+    if (!aligned(d_tets_l, 16) || !aligned(d_nbrs_l, 16))
+        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets/neighbors must be 16-byte aligned"};
+    select_device_for(d_tets_l, "tets/neighbors");
+    pb.d_labels = on_device(labels, N, l_dev, pb.dlab, s);
+    const double* d_vertices = on_device(vertices, nv * 3u, v_dev, pb.dver, s);
+    pb.d_toff = DevBuf<unsigned long long>(G + 1, s);
+    pb.d_voff = DevBuf<unsigned long long>(G + 1, s);
+    GPUPR_CUDA(cudaMemcpyAsync(pb.d_toff.p, toff, (G + 1) * 8u, cudaMemcpyHostToDevice, s));
+    GPUPR_CUDA(cudaMemcpyAsync(pb.d_voff.p, voff, (G + 1) * 8u, cudaMemcpyHostToDevice, s));
+    pb.gt = DevBuf<int32_t>(N * 4u, s);
+    pb.gn = DevBuf<int32_t>(N * 4u, s);
+    batch_pack(N, G, pb.d_toff.p, pb.d_voff.p, d_tets_l, d_nbrs_l, pb.gt.p, pb.gn.p, s, launches);
+    BuildInputs in{d_vertices, nv, pb.gt.p, pb.gn.p, pb.d_labels, N, fill_T};
+    in.want_base_node = true;
+    build_reduced_graph(in, pb.g, pb.info, s, launches);
+    if (pb.info.free_n == 0) return;
+    // each graph's free nodes form one contiguous range of reduced ids
+    DevBuf<unsigned long long> counts(G, s);
+    batch_free_counts(G, pb.d_toff.p, pb.g.full_to_free.p, counts.p, s, launches);
+    pb.hc.assign(G, 0);
+    std::vector<unsigned long long> hfo(G + 1);
+    std::vector<uint32_t> hso(G + 1);
+    GPUPR_CUDA(cudaMemcpyAsync(pb.hc.data(), counts.p, G * 8u, cudaMemcpyDeviceToHost, s));
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    hfo[0] = 0;
+    for (uint32_t k = 0; k < G; ++k) hfo[k + 1] = hfo[k] + pb.hc[k];
+    if (hfo[G] != pb.g.n) throw Error{GPUPR_ERR_INVARIANT, "batch free counts do not add up"};
+    for (uint32_t k = 0; k <= G; ++k) hso[k] = (uint32_t)hfo[k];
+    pb.d_foff = DevBuf<unsigned long long>(G + 1, s);
+    pb.d_soff = DevBuf<uint32_t>(G + 1, s);
+    GPUPR_CUDA(cudaMemcpyAsync(pb.d_foff.p, hfo.data(), (G + 1) * 8u, cudaMemcpyHostToDevice, s));
+    GPUPR_CUDA(cudaMemcpyAsync(pb.d_soff.p, hso.data(), (G + 1) * 4u, cudaMemcpyHostToDevice, s));
+    // the host vectors go out of scope: the copies must have read them
+    GPUPR_CUDA(cudaStreamSynchronize(s));
+    pb.segs.nseg = G;
+    pb.segs.d_off = pb.d_soff.p;
+}
+
+// The options of a batch's solve: the caller's fields where set; else the
+// batch tuning table's entry for the batch's size class (free nodes per
+// graph); else, for a union of at least 16 graphs averaging under 1.5M tets,
+// 8 chained hops in rounds of up to 131072 active nodes on 3 blocks per SM.
+// That rule comes from B200 measurements with 64 graphs of 50k-4M tets
+// (56.5M in all, mean 0.9M; median solve of 9 alternating runs): 73.3 ->
+// 54.7 ms on one seeded batch, 86.3 -> 90.7 ms on another, against the
+// union's own size rule; a single 5M-tet graph ran 3x slower with these
+// settings, hence the mean-size bound.
+gpupr_solve_options batch_options(const gpupr_solve_options* options, uint32_t G, uint64_t N,
+                                  uint64_t free_n)
+{
+    gpupr_solve_options o{};
+    if (options) o = *options;
+    const bool caller_set = options && (options->chain_hops > 0 || options->chain_max_active > 0 ||
+                                        options->blocks_per_sm > 0 || options->work_relabel_factor > 0);
+    if (caller_set) return o;
+    TuneEntry e;
+    if (batch_tune_lookup(free_n / (G ? G : 1u), &e)) {
+        o.blocks_per_sm = e.blocks_per_sm;
+        o.work_relabel_factor = e.work_factor;
+        o.chain_hops = e.chain_hops;
+        o.chain_max_active = e.chain_max_active;
+    } else if (G >= 16u && N / G < 1500000ull) {
+        o.chain_hops = 8;
+        o.chain_max_active = 131072;
+        o.blocks_per_sm = 3;
+    }
+    return o;
 }
 
 }  // namespace
@@ -339,42 +452,22 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     std::memset(st, 0, sizeof(*st));
     std::memset(items, 0, sizeof(gpupr_batch_item) * G);
     if (!G) return;
-    if (toff[0] != 0 || voff[0] != 0) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "batch offsets must start at 0"};
-    for (uint32_t g = 0; g < G; ++g) {
-        if (toff[g + 1] < toff[g] || voff[g + 1] < voff[g])
-            throw Error{GPUPR_ERR_INVALID_ARGUMENT, "batch offsets must be non-decreasing"};
-        items[g].n_tets = toff[g + 1] - toff[g];
-    }
-    const uint64_t N = toff[G], nv = voff[G];
+    for (uint32_t k = 0; k < G; ++k) items[k].n_tets = toff[k + 1] >= toff[k] ? toff[k + 1] - toff[k] : 0;
+    const uint64_t N = toff[G];
     st->n_full = N;
     st->threads = 1;
     st->local_steps = options && options->local_steps ? options->local_steps : 8;
-    if (N > 0x7FFFFFFEull) throw Error{GPUPR_ERR_TOO_MANY_TETS, "batch exceeds 2^31-1 tets"};
-    if (N == 0) return;
-    if (!d_tets_l || !d_nbrs_l || !labels || !out || (!vertices && nv))
-        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL batch array"};
-    if (!aligned(d_tets_l, 16) || !aligned(d_nbrs_l, 16))
-        throw Error{GPUPR_ERR_INVALID_ARGUMENT, "tets/neighbors must be 16-byte aligned"};
-    select_device_for(d_tets_l, "tets/neighbors");
+    if (N == 0 && toff[0] == 0 && voff[0] == 0) return;
+    if (!out) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL batch array"};
     uint64_t launches = 0;
 
     const auto b0 = std::chrono::steady_clock::now();
     Timer tb(s);
-    DevBuf<uint8_t> dlab;
-    DevBuf<double> dver;
-    const uint8_t* d_labels = on_device(labels, N, l_dev, dlab, s);
-    const double* d_vertices = on_device(vertices, nv * 3u, v_dev, dver, s);
-    DevBuf<unsigned long long> d_toff(G + 1, s), d_voff(G + 1, s);
-    GPUPR_CUDA(cudaMemcpyAsync(d_toff.p, toff, (G + 1) * 8u, cudaMemcpyHostToDevice, s));
-    GPUPR_CUDA(cudaMemcpyAsync(d_voff.p, voff, (G + 1) * 8u, cudaMemcpyHostToDevice, s));
-    DevBuf<int32_t> gt(N * 4u, s), gn(N * 4u, s);
-    batch_pack(N, G, d_toff.p, d_voff.p, d_tets_l, d_nbrs_l, gt.p, gn.p, s, &launches);
-
-    BuildInputs in{d_vertices, nv, gt.p, gn.p, d_labels, N, fill_T};
-    in.want_base_node = true;
-    ReducedGraph g;
-    BuildInfo info;
-    build_reduced_graph(in, g, info, s, &launches);
+    PreparedBatch pb;
+    prepare_batch(G, toff, voff, vertices, v_dev, d_tets_l, d_nbrs_l, labels, l_dev, fill_T, s, pb,
+                  &launches);
+    ReducedGraph& g = pb.g;
+    const BuildInfo& info = pb.info;
     st->build_device_ms = tb.stop_ms();
     st->build_seconds = seconds_since(b0);
     st->full_E = info.full_refs / 2u;
@@ -382,55 +475,19 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     st->fixed_sink = info.fixed_sink;
     st->free_n = info.free_n;
     if (info.free_n == 0) {
-        if (out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, d_labels, N, cudaMemcpyDeviceToDevice, s));
-        else device_to_host(out, d_labels, N, s);
+        if (out_dev) GPUPR_CUDA(cudaMemcpyAsync(out, pb.d_labels, N, cudaMemcpyDeviceToDevice, s));
+        else device_to_host(out, pb.d_labels, N, s);
         GPUPR_CUDA(cudaStreamSynchronize(s));
         st->kernel_launches = launches;
         st->native_total_seconds = seconds_since(all0);
         return;
     }
-    SolveOptions opt = resolve_options(options, 8, 1024, 2000000ull);
-    // A union of many small graphs solves like its parts: their rounds are
-    // short latency chains, so chained discharge pays in wide rounds, as it
-    // does for single graphs below 1.5M free nodes.  Measured on B200 with 64
-    // graphs of 50k-4M tets (56.5M in all, mean 0.9M; median solve of 9
-    // alternating runs): 73.3 -> 54.7 ms on one seeded batch, 86.3 -> 90.7 ms
-    // on another, with 8 hops in rounds of up to 131072 active nodes on 3
-    // blocks per SM instead of the union's size rule; a single 5M-tet graph
-    // ran 3x slower with these settings, hence the mean-size bound.  Options
-    // the caller sets win.
-    const bool caller_set = options && (options->chain_hops > 0 || options->chain_max_active > 0 ||
-                                        options->blocks_per_sm > 0);
-    if (!caller_set && G >= 16u && N / G < 1500000ull) {
-        opt.chain_hops = 8;
-        opt.chain_max_active = 131072;
-        opt.blocks_per_sm = 3;
-    }
-    // each graph's free nodes form one contiguous range of reduced ids: the
-    // segments of the solve (per-graph retirement) and of the per-graph flows
-    DevBuf<unsigned long long> counts(G, s), d_foff(G + 1, s), base(G, s);
-    DevBuf<uint32_t> d_soff(G + 1, s);
-    DevBuf<long long> raw(G, s);
-    batch_free_counts(G, d_toff.p, g.full_to_free.p, counts.p, s, &launches);
-    std::vector<unsigned long long> hc(G), hfo(G + 1), hb(G);
-    std::vector<uint32_t> hso(G + 1);
-    std::vector<long long> hr(G);
-    GPUPR_CUDA(cudaMemcpyAsync(hc.data(), counts.p, G * 8u, cudaMemcpyDeviceToHost, s));
-    GPUPR_CUDA(cudaStreamSynchronize(s));
-    hfo[0] = 0;
-    for (uint32_t k = 0; k < G; ++k) hfo[k + 1] = hfo[k] + hc[k];
-    if (hfo[G] != g.n) throw Error{GPUPR_ERR_INVARIANT, "batch free counts do not add up"};
-    for (uint32_t k = 0; k <= G; ++k) hso[k] = (uint32_t)hfo[k];
-    GPUPR_CUDA(cudaMemcpyAsync(d_foff.p, hfo.data(), (G + 1) * 8u, cudaMemcpyHostToDevice, s));
-    GPUPR_CUDA(cudaMemcpyAsync(d_soff.p, hso.data(), (G + 1) * 4u, cudaMemcpyHostToDevice, s));
-    Segments segs;
-    segs.nseg = G;
-    segs.d_off = d_soff.p;
-
+    const gpupr_solve_options bo = batch_options(options, G, N, info.free_n);
+    SolveOptions opt = resolve_options(&bo, 8, 1024, 2000000ull);
     opt.max_blocks_per_sm = max_blocks_per_sm;
     SolveWorkspace w;
     SolveResult sr;
-    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr, &segs);
+    solve_push_relabel(g.n, g.nbr.p, g.res.p, g.rev.p, g.pair.p, g.term.p, w, opt, s, sr, &pb.segs);
     launches += sr.launches;
 
     DevBuf<uint8_t> dout;
@@ -439,11 +496,15 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
         dout = DevBuf<uint8_t>(N, s);
         d_out = dout.p;
     }
-    GPUPR_CUDA(cudaMemcpyAsync(d_out, d_labels, N, cudaMemcpyDeviceToDevice, s));
+    GPUPR_CUDA(cudaMemcpyAsync(d_out, pb.d_labels, N, cudaMemcpyDeviceToDevice, s));
     scatter_partition(g.n, g.free_old.p, w.height.p, d_out, s, &launches);
 
     // per-graph flows over each graph's contiguous free-node range
-    batch_flows(G, d_foff.p, g.term.p, w.excess.p, g.base_node.p, raw.p, base.p, s, &launches);
+    DevBuf<unsigned long long> base(G, s);
+    DevBuf<long long> raw(G, s);
+    std::vector<unsigned long long> hb(G);
+    std::vector<long long> hr(G);
+    batch_flows(G, pb.d_foff.p, g.term.p, w.excess.p, g.base_node.p, raw.p, base.p, s, &launches);
     GPUPR_CUDA(cudaMemcpyAsync(hr.data(), raw.p, G * 8u, cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaMemcpyAsync(hb.data(), base.p, G * 8u, cudaMemcpyDeviceToHost, s));
     if (!out_dev) device_to_host(out, d_out, N, s);
@@ -451,7 +512,7 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     for (uint32_t k = 0; k < G; ++k) {
         items[k].raw_flow = hr[k];
         items[k].adjusted_flow = hr[k] + (long long)hb[k];
-        items[k].free_n = hc[k];
+        items[k].free_n = pb.hc[k];
     }
     st->raw_flow = sr.raw_flow;
     st->adjusted_flow = sr.raw_flow + info.terminal_base_flow;
@@ -480,6 +541,36 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     st->bottom_up_steps = sr.bottom_up_steps;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
+}
+
+// gpupr_autotune_batch: one pack and build, then the two-stage tuning of the
+// segmented solve against the batch rule; the entry is kept for the batch's
+// size class (free nodes per graph).
+TuneEntry run_autotune_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
+                             const double* vertices, int v_dev, const int32_t* d_tets_l,
+                             const int32_t* d_nbrs_l, const uint8_t* labels, int l_dev, double fill_T,
+                             int32_t local_steps, int32_t reps, cudaStream_t s)
+{
+    if (!G || !toff || !voff) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "NULL batch argument"};
+    if (reps <= 0) reps = 3;
+    if (reps > 50) reps = 50;
+    uint64_t launches = 0;
+    PreparedBatch pb;
+    prepare_batch(G, toff, voff, vertices, v_dev, d_tets_l, d_nbrs_l, labels, l_dev, fill_T, s, pb,
+                  &launches);
+    if (pb.info.free_n == 0) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "autotune: the batch has no free tet"};
+    const uint64_t mean_free = pb.info.free_n / G;
+    // the rule, not an older entry of this class
+    std::vector<TuneEntry> keep = batch_tune_all();
+    keep.erase(std::remove_if(keep.begin(), keep.end(),
+                              [&](const TuneEntry& e) { return e.size_class == size_class((uint32_t)mean_free); }),
+               keep.end());
+    batch_tune_replace(keep);
+    const gpupr_solve_options base = batch_options(nullptr, G, toff[G], pb.info.free_n);
+    TuneEntry best = two_stage_tune(pb.g, &pb.segs, base, local_steps, reps, s);
+    best.size_class = size_class((uint32_t)mean_free);
+    batch_tune_store(best);
+    return best;
 }
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
@@ -945,40 +1036,82 @@ gpupr_status gpupr_autotune(const double* vertices, uint64_t n_vertices, int ver
     });
 }
 
+namespace {
+void export_entries(const std::vector<gpupr::TuneEntry>& all, gpupr_tune_entry* entries,
+                    uint32_t capacity, uint32_t* count)
+{
+    *count = (uint32_t)all.size();
+    for (uint32_t i = 0; i < all.size() && i < capacity && entries; ++i) {
+        entries[i].size_class = all[i].size_class;
+        entries[i].blocks_per_sm = all[i].blocks_per_sm;
+        entries[i].work_relabel_factor = all[i].work_factor;
+        entries[i].solve_ms = all[i].solve_ms;
+        entries[i].default_ms = all[i].default_ms;
+        entries[i].chain_hops = all[i].chain_hops;
+        entries[i].chain_max_active = all[i].chain_max_active;
+    }
+}
+
+std::vector<gpupr::TuneEntry> import_entries(const gpupr_tune_entry* entries, uint32_t count)
+{
+    if (count && !entries) throw gpupr::Error{GPUPR_ERR_INVALID_ARGUMENT, "entries pointer is NULL"};
+    std::vector<gpupr::TuneEntry> v(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        v[i].size_class = entries[i].size_class;
+        v[i].blocks_per_sm = entries[i].blocks_per_sm;
+        v[i].work_factor = entries[i].work_relabel_factor;
+        v[i].solve_ms = entries[i].solve_ms;
+        v[i].default_ms = entries[i].default_ms;
+        v[i].chain_hops = entries[i].chain_hops;
+        v[i].chain_max_active = entries[i].chain_max_active;
+    }
+    return v;
+}
+}  // namespace
+
 gpupr_status gpupr_tune_table(gpupr_tune_entry* entries, uint32_t capacity, uint32_t* count)
 {
     return guarded([&] {
         if (!count) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "count pointer is NULL"};
-        const std::vector<TuneEntry> all = tune_all();
-        *count = (uint32_t)all.size();
-        for (uint32_t i = 0; i < all.size() && i < capacity && entries; ++i) {
-            entries[i].size_class = all[i].size_class;
-            entries[i].blocks_per_sm = all[i].blocks_per_sm;
-            entries[i].work_relabel_factor = all[i].work_factor;
-            entries[i].solve_ms = all[i].solve_ms;
-            entries[i].default_ms = all[i].default_ms;
-            entries[i].chain_hops = all[i].chain_hops;
-            entries[i].chain_max_active = all[i].chain_max_active;
-        }
+        export_entries(tune_all(), entries, capacity, count);
     });
 }
 
 gpupr_status gpupr_tune_table_set(const gpupr_tune_entry* entries, uint32_t count)
 {
+    return guarded([&] { tune_replace(import_entries(entries, count)); });
+}
+
+gpupr_status gpupr_autotune_batch(uint32_t n_graphs, const uint64_t* tet_offsets,
+                                  const uint64_t* vertex_offsets, const double* vertices,
+                                  int vertices_on_device, const int32_t* d_tets,
+                                  const int32_t* d_neighbors, const uint8_t* labels,
+                                  int labels_on_device, double fill_T, int32_t local_steps,
+                                  int32_t reps, gpupr_tune_entry* chosen, void* stream)
+{
     return guarded([&] {
-        if (count && !entries) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "entries pointer is NULL"};
-        std::vector<TuneEntry> v(count);
-        for (uint32_t i = 0; i < count; ++i) {
-            v[i].size_class = entries[i].size_class;
-            v[i].blocks_per_sm = entries[i].blocks_per_sm;
-            v[i].work_factor = entries[i].work_relabel_factor;
-            v[i].solve_ms = entries[i].solve_ms;
-            v[i].default_ms = entries[i].default_ms;
-            v[i].chain_hops = entries[i].chain_hops;
-            v[i].chain_max_active = entries[i].chain_max_active;
+        const TuneEntry e = run_autotune_batch(n_graphs, tet_offsets, vertex_offsets, vertices,
+                                               vertices_on_device, d_tets, d_neighbors, labels,
+                                               labels_on_device, fill_T, local_steps > 0 ? local_steps : 8,
+                                               reps, static_cast<cudaStream_t>(stream));
+        if (chosen) {
+            uint32_t one = 0;
+            export_entries({e}, chosen, 1, &one);
         }
-        tune_replace(v);
     });
+}
+
+gpupr_status gpupr_batch_tune_table(gpupr_tune_entry* entries, uint32_t capacity, uint32_t* count)
+{
+    return guarded([&] {
+        if (!count) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "count pointer is NULL"};
+        export_entries(batch_tune_all(), entries, capacity, count);
+    });
+}
+
+gpupr_status gpupr_batch_tune_table_set(const gpupr_tune_entry* entries, uint32_t count)
+{
+    return guarded([&] { batch_tune_replace(import_entries(entries, count)); });
 }
 
 gpupr_status gpupr_release_cached_memory(void)

@@ -316,6 +316,11 @@ void tune_store(const TuneEntry& e);
 std::vector<TuneEntry> tune_all();
 void tune_replace(const std::vector<TuneEntry>& entries);
 int size_class(uint32_t n);
+// The batch table, by the size class of the free nodes per graph.
+bool batch_tune_lookup(uint64_t mean_free, TuneEntry* out);
+void batch_tune_store(const TuneEntry& e);
+std::vector<TuneEntry> batch_tune_all();
+void batch_tune_replace(const std::vector<TuneEntry>& entries);
 
 // Phase-I push-relabel on a reduced graph (res/term updated in place).
 // On return the workspace heights mark the sink-reachable set

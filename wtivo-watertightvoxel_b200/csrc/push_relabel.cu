@@ -1613,18 +1613,61 @@ void solve_reduced_noalloc(uint32_t n, int32_t* d_nbr, uint32_t* d_res, int32_t*
 }
 
 // ---------------------------------------------------------------------------
-// Autotuner table: one entry per size class, shared by the process.
+// Autotuner tables: one entry per size class, shared by the process; one
+// table for single graphs (class of the free-node count) and one for batches
+// (class of the free nodes per graph).
 // ---------------------------------------------------------------------------
 namespace {
-std::mutex g_tune_mu;
-TuneEntry g_tune[33];
-bool g_tune_valid[33] = {};
+struct TuneTable {
+    std::mutex mu;
+    TuneEntry e[33];
+    bool valid[33] = {};
+};
+TuneTable g_tune, g_batch_tune;
 
 bool valid_entry(const TuneEntry& e)
 {
     return e.size_class >= 0 && e.size_class <= 32 && e.blocks_per_sm >= 1 && e.blocks_per_sm <= 32 &&
            e.work_factor > 0.0 && e.work_factor < 1e6 && e.chain_hops >= 1 && e.chain_hops <= 64 &&
            e.chain_max_active >= 1;
+}
+
+bool table_lookup(TuneTable& t, uint32_t n, TuneEntry* out)
+{
+    std::lock_guard<std::mutex> lk(t.mu);
+    const int k = size_class(n);
+    if (!t.valid[k]) return false;
+    *out = t.e[k];
+    return true;
+}
+
+void table_store(TuneTable& t, const TuneEntry& e)
+{
+    if (!valid_entry(e)) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "invalid tuning entry"};
+    std::lock_guard<std::mutex> lk(t.mu);
+    t.e[e.size_class] = e;
+    t.valid[e.size_class] = true;
+}
+
+std::vector<TuneEntry> table_all(TuneTable& t)
+{
+    std::lock_guard<std::mutex> lk(t.mu);
+    std::vector<TuneEntry> v;
+    for (int k = 0; k <= 32; ++k)
+        if (t.valid[k]) v.push_back(t.e[k]);
+    return v;
+}
+
+void table_replace(TuneTable& t, const std::vector<TuneEntry>& entries)
+{
+    for (const TuneEntry& e : entries)
+        if (!valid_entry(e)) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "invalid tuning entry"};
+    std::lock_guard<std::mutex> lk(t.mu);
+    for (int k = 0; k <= 32; ++k) t.valid[k] = false;
+    for (const TuneEntry& e : entries) {
+        t.e[e.size_class] = e;
+        t.valid[e.size_class] = true;
+    }
 }
 }  // namespace
 
@@ -1635,42 +1678,17 @@ int size_class(uint32_t n)
     return k;
 }
 
-bool tune_lookup(uint32_t n, TuneEntry* out)
-{
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    const int k = size_class(n);
-    if (!g_tune_valid[k]) return false;
-    *out = g_tune[k];
-    return true;
-}
+bool tune_lookup(uint32_t n, TuneEntry* out) { return table_lookup(g_tune, n, out); }
+void tune_store(const TuneEntry& e) { table_store(g_tune, e); }
+std::vector<TuneEntry> tune_all() { return table_all(g_tune); }
+void tune_replace(const std::vector<TuneEntry>& entries) { table_replace(g_tune, entries); }
 
-void tune_store(const TuneEntry& e)
+bool batch_tune_lookup(uint64_t mean_free, TuneEntry* out)
 {
-    if (!valid_entry(e)) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "invalid tuning entry"};
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[e.size_class] = e;
-    g_tune_valid[e.size_class] = true;
+    return table_lookup(g_batch_tune, (uint32_t)std::min<uint64_t>(mean_free, 0xFFFFFFFFull), out);
 }
-
-std::vector<TuneEntry> tune_all()
-{
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    std::vector<TuneEntry> v;
-    for (int k = 0; k <= 32; ++k)
-        if (g_tune_valid[k]) v.push_back(g_tune[k]);
-    return v;
-}
-
-void tune_replace(const std::vector<TuneEntry>& entries)
-{
-    for (const TuneEntry& e : entries)
-        if (!valid_entry(e)) throw Error{GPUPR_ERR_INVALID_ARGUMENT, "invalid tuning entry"};
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    for (int k = 0; k <= 32; ++k) g_tune_valid[k] = false;
-    for (const TuneEntry& e : entries) {
-        g_tune[e.size_class] = e;
-        g_tune_valid[e.size_class] = true;
-    }
-}
+void batch_tune_store(const TuneEntry& e) { table_store(g_batch_tune, e); }
+std::vector<TuneEntry> batch_tune_all() { return table_all(g_batch_tune); }
+void batch_tune_replace(const std::vector<TuneEntry>& entries) { table_replace(g_batch_tune, entries); }
 
 }  // namespace gpupr

@@ -520,6 +520,45 @@ def autotune(vertices, tets, nbrs, labels, fill_T, local_steps=8, reps=3):
     return {k: getattr(e, k) for k, _ in TuneEntry._fields_}
 
 
+def autotune_batch(toff, voff, vertices, tets, nbrs, labels, fill_T, local_steps=8, reps=3):
+    """gpupr_autotune_batch on one packed batch (arguments as graph_cut_batch):
+    returns the chosen entry of the batch's size bucket as a dict."""
+    import torch
+
+    G = len(toff) - 1
+    toff = np.ascontiguousarray(toff, np.uint64)
+    voff = np.ascontiguousarray(voff, np.uint64)
+    v_dev = isinstance(vertices, torch.Tensor)
+    l_dev = isinstance(labels, torch.Tensor)
+    if not v_dev:
+        vertices = np.ascontiguousarray(vertices, np.float64)
+    if not l_dev:
+        labels = np.ascontiguousarray(labels, np.uint8)
+    e = TuneEntry()
+    check(lib().gpupr_autotune_batch(G, _hp(toff), _hp(voff), _dp(vertices) if v_dev else _hp(vertices),
+                                     int(v_dev), _dp(tets), _dp(nbrs), _dp(labels) if l_dev else _hp(labels),
+                                     int(l_dev), float(fill_T), int(local_steps), int(reps), ctypes.byref(e),
+                                     _stream(torch, tets.device)))
+    return {k: getattr(e, k) for k, _ in TuneEntry._fields_}
+
+
+def batch_tune_table():
+    """The batch tuning table as a list of dicts."""
+    cnt = ctypes.c_uint32(0)
+    check(lib().gpupr_batch_tune_table(None, 0, ctypes.byref(cnt)))
+    arr = (TuneEntry * max(cnt.value, 1))()
+    check(lib().gpupr_batch_tune_table(arr, cnt.value, ctypes.byref(cnt)))
+    return [{k: getattr(arr[i], k) for k, _ in TuneEntry._fields_} for i in range(cnt.value)]
+
+
+def set_batch_tune_table(entries):
+    arr = (TuneEntry * max(len(entries), 1))()
+    for i, e in enumerate(entries):
+        for k, _ in TuneEntry._fields_:
+            setattr(arr[i], k, e[k])
+    check(lib().gpupr_batch_tune_table_set(arr, len(entries)))
+
+
 def tune_table():
     n = ctypes.c_uint32(0)
     check(lib().gpupr_tune_table(None, 0, ctypes.byref(n)))
