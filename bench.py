@@ -98,15 +98,16 @@ def parse():
     ap.add_argument("--raw-seeds", type=int, default=16)
     ap.add_argument("--no-raw-check", action="store_true",
                     help="skip the full-size BK check of the first raw seed")
-    ap.add_argument("--only", default="", help="comma list of extra legs to run: " + ",".join(LEGS))
+    ap.add_argument("--only", default="", help="comma list of extra legs to run: " + ",".join(LEGS)
+                    + " ('cut' alone: the timed cut and no extra leg)")
     a = ap.parse_args()
     only = {x.strip() for x in a.only.split(",") if x.strip()}
-    bad = only - set(LEGS)
+    bad = only - set(LEGS) - {"cut"}
     if bad:
         ap.error(f"unknown legs {sorted(bad)}")
     off = {"e2e": a.no_e2e, "cpu": a.no_cpu_baseline, "batch": a.no_batch, "serve": a.no_serve,
            "labels": a.no_labels, "audit": a.no_audit, "raw": a.no_raw, "autotune": a.no_autotune}
-    a.legs = (only if only else set(LEGS)) - {k for k, v in off.items() if v}
+    a.legs = ((only - {"cut"}) if only else set(LEGS)) - {k for k, v in off.items() if v}
     return a
 
 
