@@ -67,9 +67,12 @@ WORKLOAD = "torus-knot (3,5) tube, 2% patches dropped, inner shell 0.002, noise 
 # algorithmic bytes per unit of the solver: a discharge node visit
 # reads nbr 16 + res 16 + rev 1 + term 4 + excess 8 + height 4 + 4 neighbour
 # heights 16, queue read+write 8 = 73 B; each push adds res+reverse res 8 and
-# two excess updates 16 = 24 B; a BFS frontier expansion reads nbr 16 + rev 1
-# + 4 heights 16 + 4 reverse residuals 16 and writes height+queue 8 = 57 B.
-B_VISIT, B_PUSH, B_BFS = 73, 24, 57
+# two excess updates 16 = 24 B; a BFS frontier expansion reads the node's
+# in-arc row 16 + 4 neighbour heights 16 and writes a label + queue entry 8 =
+# 40 B; every global relabel streams over each node twice: the seed (term 4,
+# height write 4, nbr 16 + pair 16 + res 16 read and the in-arc row 16
+# written) and the active sweep (height 4 + excess 8) = 84 B.
+B_VISIT, B_PUSH, B_BFS, B_SWEEP = 73, 24, 40, 84
 
 
 LEGS = ("e2e", "cpu", "batch", "serve", "labels", "audit", "raw", "config1", "noalloc", "autotune",
@@ -333,7 +336,8 @@ def run_ours(args, world, rank, local):
         # persistent engine: one cooperative launch holds every round and
         # every BFS level; its duration is the solve's device time
         kern = "k_solve_persistent"
-        nbytes = B_VISIT * visits + B_PUSH * pushes + B_BFS * bfsv
+        sweeps = sum(int(s["global_relabels"]) * int(s["free_n"]) for s in stats)
+        nbytes = B_VISIT * visits + B_PUSH * pushes + B_BFS * bfsv + B_SWEEP * sweeps
         kms, launches = sum(s["solve_device_ms"] for s in stats), len(stats)
     elif dis_ms >= bfs_ms:
         kern = "k_discharge"

@@ -84,10 +84,15 @@ def test_batch_retires_finished_graphs(built):
     """Graphs of very different size finish at different relabels: the small
     ones retire while the large one still runs, and every graph keeps exactly
     its own cut (its labels from the relabel at which it retired)."""
+    import gpupr_capi
+
     graphs = [cached_graph("lattice", 2, 80_000)] + [cached_graph("proxy", s, 6_000) for s in range(6)] + \
              [cached_graph("lattice", 3, 300_000)]
-    toff, (out, items, st) = _run_batch(graphs)
-    assert st["engine"] == 2 and st["graphs_retired"] >= 1
+    # a relabel every 16 discharge rounds: the small graphs finish after a few
+    # relabels while the large one needs many more
+    toff, (out, items, st) = _run_batch(graphs, opts=gpupr_capi.options(engine=2, global_relabel_period=16,
+                                                                        chain_hops=1))
+    assert st["engine"] == 2 and st["global_relabels"] > 2 and st["graphs_retired"] >= 1
     for k, g in enumerate(graphs):
         lab, ost = orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0)
         assert np.array_equal(out[int(toff[k]):int(toff[k + 1])], lab), k

@@ -74,6 +74,10 @@ struct SolveView {
                                         // arc pair's residual sum (u = nbr[v][k]); a push
                                         // moves residual between the two arcs and keeps it,
                                         // so r(u->v) = pair - res[v][k] between phases
+    int4* inrow;                        // [n] persistent engine: per node the neighbours
+                                        // with a residual arc into it (-1 elsewhere),
+                                        // written by each relabel's seed sweep (null:
+                                        // the BFS derives them from pair and res)
     int32_t* term;                      // [n] src - snk residual
     long long* excess;                  // [n]
     uint32_t* height;                   // [n]
@@ -274,10 +278,12 @@ struct SolveWorkspace {
     DevBuf<Ctl> ctl;
     DevBuf<uint32_t> chunk_seg, seg_live, seg_act;   // segmented solves only
     DevBuf<uint32_t> cand0, cand1;                   // direction-optimizing relabels only
+    DevBuf<int4> inrow;                              // persistent engine: in-arc rows
     uint64_t bytes() const
     {
         return excess.bytes() + height.bytes() + q0.bytes() + q1.bytes() + q2.bytes() + ctl.bytes() +
-               chunk_seg.bytes() + seg_live.bytes() + seg_act.bytes() + cand0.bytes() + cand1.bytes();
+               chunk_seg.bytes() + seg_live.bytes() + seg_act.bytes() + cand0.bytes() + cand1.bytes() +
+               inrow.bytes();
     }
 };
 

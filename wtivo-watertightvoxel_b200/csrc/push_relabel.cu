@@ -139,8 +139,21 @@ __device__ __forceinline__ bool sweep_node(const SolveView& g, uint32_t seg0, ui
     return ldcg(g.seg_live + *seg) != 0u;
 }
 
+// The neighbours v of node u with a residual arc v -> u, as a row (-1 where
+// there is none): r(v->u) = pair[u][k] - res[u][k], exact between phases.
+__device__ __forceinline__ int4 in_arc_row(const SolveView& g, uint32_t u)
+{
+    const int4 nb4 = __ldg(g.nbr + u);
+    const uint4 p4 = __ldg(g.pair + u);
+    const uint4 r4 = __ldcg(reinterpret_cast<const uint4*>(g.res) + u);
+    return make_int4(p4.x > r4.x ? nb4.x : -1, p4.y > r4.y ? nb4.y : -1, p4.z > r4.z ? nb4.z : -1,
+                     p4.w > r4.w ? nb4.w : -1);
+}
+
 // Level 1 of the backward BFS: nodes with a residual arc to the sink.  Every
-// other height is reset to UNVIS (.cu:374-379).  s_m[0..5] are the block's
+// other height is reset to UNVIS (.cu:374-379).  With g.inrow (persistent
+// engine) the same streaming pass writes every node's in-arc row, so a BFS
+// step reads one 16-byte row per frontier node instead of three.  s_m[0..5] are the block's
 // staging counters (frontier count, active count, and their flush copies);
 // s_fr and s_act hold DTPB * SWEEP_UNROLL entries each.  With kActive the
 // seeds that hold excess are appended to the active queue (engine 1; the
@@ -168,6 +181,13 @@ __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr
             const uint32_t v = base + j * DTPB + threadIdx.x;
             x[j] = (kActive && in[j] && t[j] < 0) ? ldcg(g.excess + v) : 0ll;
             if (in[j]) g.height[v] = (t[j] < 0) ? 1u : UNVIS;
+        }
+        if (g.inrow) {
+#pragma unroll 2
+            for (int j = 0; j < SWEEP_UNROLL; ++j) {
+                const uint32_t v = base + j * DTPB + threadIdx.x;
+                if (in[j]) __stcg(g.inrow + v, in_arc_row(g, v));
+            }
         }
 #pragma unroll
         for (int j = 0; j < SWEEP_UNROLL; ++j) {
@@ -282,12 +302,12 @@ __device__ __forceinline__ uint32_t prefetch_entry(const uint32_t* in, uint32_t 
 // push is in flight).  Returns u's neighbour row; bit k of *arcs is slot k.
 __device__ __forceinline__ int4 residual_in_arcs(const SolveView& g, uint32_t u, uint32_t* arcs)
 {
-    const int4 nb4 = __ldg(g.nbr + u);
-    const uint4 p4 = __ldg(g.pair + u);
-    const uint4 r4 = __ldcg(reinterpret_cast<const uint4*>(g.res) + u);
-    *arcs = (uint32_t)(nb4.x >= 0 && p4.x > r4.x) | ((uint32_t)(nb4.y >= 0 && p4.y > r4.y) << 1) |
-            ((uint32_t)(nb4.z >= 0 && p4.z > r4.z) << 2) | ((uint32_t)(nb4.w >= 0 && p4.w > r4.w) << 3);
-    return nb4;
+    // the row this relabel's seed sweep wrote (L2: written by other blocks), or
+    // derived from u's own rows
+    const int4 r = g.inrow ? __ldcg(g.inrow + u) : in_arc_row(g, u);
+    *arcs = (uint32_t)(r.x >= 0) | ((uint32_t)(r.y >= 0) << 1) | ((uint32_t)(r.z >= 0) << 2) |
+            ((uint32_t)(r.w >= 0) << 3);
+    return r;
 }
 
 // One top-down BFS level L over cnt frontier nodes: each frontier node u
@@ -1276,6 +1296,9 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
             g.seg_act = w.seg_act.p;
             out.workspace_bytes = w.bytes();
         }
+        if (w.inrow.n < n) w.inrow = DevBuf<int4>(n, s);
+        g.inrow = w.inrow.p;
+        out.workspace_bytes = w.bytes();
         if (opt.bfs_bottom_up) {
             if (w.cand0.n < n) {
                 w.cand0 = DevBuf<uint32_t>(n, s);
