@@ -659,7 +659,24 @@ def run_raw(args, local):
         check = {"seed": args.seed, "identical_to_oracle": bool(
                      f_bk + int(np.minimum(src, snk).sum()) == res[0][0]
                      and np.array_equal(res[0][1].cpu().numpy(), p_bk)),
-                 "oracle_s": round(cpu_s, 2)}
+                 "oracle_s": round(cpu_s, 2),
+                 "source_side_nodes": int(sizes[0] - int(res[0][1].sum().item()))}
+        # the workload's n-links (1e4 x area / mean) dwarf the t-links, so its
+        # minimum cut takes every source t-link; the same graph with n-links of
+        # 30 x area / mean cuts along the sphere: checked against BK as well
+        gw = synth.config4(args.seed, n_points=2_000_000, use_delaunay=False, nlink_scale=30.0)
+        dw = tuple(torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+                   for x in (gw["nbr"], gw["cap"].view(np.int32), gw["src"].view(np.int32),
+                             gw["snk"].view(np.int32)))
+        fw, pw, stw = gpupr_capi.solve_ell(*dw)
+        sw, kw = gw["src"].astype(np.int64), gw["snk"].astype(np.int64)
+        fbw, _, _, pbw = orc.maxflow_bk(gw["nbr"], gw["cap"], (sw - kw).astype(np.int32))
+        check["weak_nlinks_30"] = {
+            "identical_to_oracle": bool(fbw + int(np.minimum(sw, kw).sum()) == fw
+                                        and np.array_equal(pw.cpu().numpy(), pbw)),
+            "source_side_nodes": int(len(pbw) - int(pbw.sum())), "flow": int(fw),
+            "solve_device_ms": round(stw["solve_device_ms"], 3)}
+        del dw, gw
         cpu = {"value": round(sizes[0] / cpu_s, 1), "unit": "nodes/s", "cores": 1, "kind": "port",
                "sample": f"seed {args.seed}, {sizes[0]} nodes: BK max flow + partition, "
                          "oracle/wtivo_oracle.c", "host": host_cpu()}

@@ -166,3 +166,14 @@ def test_python_structs_match_the_header(tmp_path):
         assert int(got[cname]) == ctypes.sizeof(py), cname
         for f, _ in py._fields_:
             assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, (cname, f)
+
+
+def test_every_header_function_has_argtypes(built):
+    """The ctypes binding declares argument types for every function the
+    header declares (an undeclared one would be called with guessed types)."""
+    import gpupr_capi
+
+    L = gpupr_capi.lib()
+    missing = [n for n in gpupr_capi.header_functions()
+               if getattr(L, n).argtypes is None and n not in ("gpupr_abi_version",)]
+    assert not missing, missing

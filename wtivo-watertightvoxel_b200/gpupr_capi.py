@@ -142,6 +142,10 @@ def lib():
                                      f64, ctypes.c_int32, ctypes.c_int32, p, p]
         L.gpupr_tune_table.argtypes = [p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
         L.gpupr_tune_table_set.argtypes = [p, ctypes.c_uint32]
+        L.gpupr_autotune_batch.argtypes = [ctypes.c_uint32, p, p, p, ctypes.c_int, p, p, p, ctypes.c_int,
+                                           f64, ctypes.c_int32, ctypes.c_int32, p, p]
+        L.gpupr_batch_tune_table.argtypes = [p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+        L.gpupr_batch_tune_table_set.argtypes = [p, ctypes.c_uint32]
         L.gpupr_release_cached_memory.argtypes = []
         L.gpupr_selftest_bounded_wait.argtypes = [ctypes.c_uint32, p]
         for name in header_functions():

@@ -68,7 +68,7 @@ def _L():
                                        ctypes.c_int64, p, ctypes.c_int64, p, p,
                                        ctypes.c_double, p]
         L.synth_udf_labels.restype = ctypes.c_int
-        L.synth_raw_graph.argtypes = [p, p, p, ctypes.c_int64, p, p, p, p, p]
+        L.synth_raw_graph.argtypes = [p, p, p, ctypes.c_int64, p, ctypes.c_double, p, p, p, p]
         L.synth_raw_graph.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -513,11 +513,13 @@ def config3_graph(i: int, n_tets: int, seed: int = 0):
     return g
 
 
-def config4(seed: int = 0, n_points: int = 2_000_000, use_delaunay: bool = True):
+def config4(seed: int = 0, n_points: int = 2_000_000, use_delaunay: bool = True,
+            nlink_scale: float = 1e4):
     """Integer-capacity raw graph: uniform points in [0,1]^3, n-link
-    round(1e4*area/mean_area) (symmetric per face), t-links from a noisy
-    sphere SDF (c=0.5, r=0.3, sigma=0.02): src=round(100*max(0,-d')),
-    snk=round(100*max(0,d')).  Returns dict(nbr, cap, src, snk)."""
+    round(nlink_scale*area/mean_area) (symmetric per face; 1e4 in the
+    workload), t-links from a noisy sphere SDF (c=0.5, r=0.3, sigma=0.02):
+    src=round(100*max(0,-d')), snk=round(100*max(0,d')).  Returns
+    dict(nbr, cap, src, snk)."""
     rng = np.random.default_rng(seed)
     if use_delaunay:
         P = rng.random((n_points, 3))
@@ -525,11 +527,11 @@ def config4(seed: int = 0, n_points: int = 2_000_000, use_delaunay: bool = True)
     else:
         m = max(2, int(round(n_points ** (1.0 / 3.0))) - 1)
         P, tets, nbrs = lattice_cells((m, m, m), (0, 0, 0), (1, 1, 1), seed=seed)
-    return raw_graph_from_cells(P, tets, nbrs, rng)
+    return raw_graph_from_cells(P, tets, nbrs, rng, nlink_scale)
 
 
-def raw_graph_from_cells(P, tets, nbrs, rng):
-    """Integer n-links round(1e4*area/mean_area), identical in both
+def raw_graph_from_cells(P, tets, nbrs, rng, nlink_scale: float = 1e4):
+    """Integer n-links round(nlink_scale*area/mean_area), identical in both
     directions (each face's area is taken from its lower-id tet), and sphere
     SDF t-links with Gaussian noise (sigma 0.02) drawn from rng
     (synth_raw_graph in synth.c)."""
@@ -542,8 +544,8 @@ def raw_graph_from_cells(P, tets, nbrs, rng):
     cap = np.empty((N, 4), np.uint32)
     src = np.empty(N, np.uint32)
     snk = np.empty(N, np.uint32)
-    rc = _L().synth_raw_graph(_ptr(P), _ptr(tets), _ptr(nbrs), N, _ptr(noise), _ptr(scratch),
-                              _ptr(cap), _ptr(src), _ptr(snk))
+    rc = _L().synth_raw_graph(_ptr(P), _ptr(tets), _ptr(nbrs), N, _ptr(noise), float(nlink_scale),
+                              _ptr(scratch), _ptr(cap), _ptr(src), _ptr(snk))
     if rc != 0:
         raise ValueError("raw_graph_from_cells: asymmetric neighbours" if rc == -1 else "out of memory")
     return dict(nbr=nbrs, cap=cap, src=src, snk=snk, n_points=len(P))

@@ -411,8 +411,9 @@ int synth_brick_udf(const double* MV, int64_t nv, const int32_t* MF, int64_t nf,
 
 /*
  * synth_raw_graph: the integer-capacity raw graph of a tet mesh (all cells
- * free, CelloCut slots).  n-link of slot k of tet i = rint(1e4 * area /
- * mean_area), where area is the face's area taken from the face's lower-id
+ * free, CelloCut slots).  n-link of slot k of tet i = rint(scale * area /
+ * mean_area) (scale 1e4 in the integer-graph workload), where area is the
+ * face's area taken from the face's lower-id
  * tet, so both directions of a face carry the same capacity, and mean_area
  * is the mean over every slot with a neighbour.  t-links from the signed
  * distance of the centroid (mean of the 4 vertices) to the sphere of centre
@@ -422,8 +423,8 @@ int synth_brick_udf(const double* MV, int64_t nv, const int32_t* MF, int64_t nf,
  * count.  Returns 0, or -1 when a neighbour does not list the tet back.
  */
 int synth_raw_graph(const double* P, const int32_t* tets, const int32_t* nbrs, int64_t N,
-                    const double* noise, double* area_scratch, uint32_t* cap, uint32_t* src,
-                    uint32_t* snk)
+                    const double* noise, double scale, double* area_scratch, uint32_t* cap,
+                    uint32_t* src, uint32_t* snk)
 {
     static const int lut[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
     const int64_t BLK = 65536;
@@ -472,7 +473,7 @@ int synth_raw_graph(const double* P, const int32_t* tets, const int32_t* nbrs, i
                 if (rk < 0) { bad = 1; rk = 0; }
                 fa = area_scratch[4 * (int64_t)j + rk];
             }
-            cap[4 * i + f] = (uint32_t)rint(1e4 * fa / mean);
+            cap[4 * i + f] = (uint32_t)rint(scale * fa / mean);
         }
         double c[3] = {0.0, 0.0, 0.0};
         for (int k = 0; k < 4; ++k)
