@@ -454,7 +454,7 @@ gpupr_status gpupr_sample_tet_labels(const gpupr_brick_grid* grid, const double*
  * builds the reduced graph of the given cut once, then times the solve
  * (restoring the graph each time), `reps` times each (default 3),
  * interleaved: first every pair of blocks per SM {1,2,3,4} and work factor
- * {0.5,1,2}, then, with the best pair, chaining off, 4 hops up to 4096 or
+ * {0.25,0.5,1,2}, then, with the best pair, chaining off, 4 hops up to 4096 or
  * 32768 active nodes, 8 hops up to 131072, beside the built-in rule.  The
  * setting with the lowest median (the rule's own values when it wins) is
  * kept for the graph's size class (free nodes in [2^k, 2^(k+1))).  Later solves whose options leave those fields at 0 use

@@ -23,7 +23,7 @@ def test_autotune_then_cut(built):
     e = gpupr_capi.autotune(g["vertices"], tets, nbrs, g["labels"], g["fill_T"], reps=2)
     k = int(st0["free_n"]).bit_length() - 1
     assert e["size_class"] == k
-    assert e["blocks_per_sm"] in (1, 2, 3, 4) and e["work_relabel_factor"] in (0.5, 1.0, 2.0)
+    assert e["blocks_per_sm"] in (1, 2, 3, 4) and e["work_relabel_factor"] in (0.25, 0.5, 1.0, 2.0)
     assert 0 < e["solve_ms"] <= e["default_ms"] * 1.5
     assert [t["size_class"] for t in gpupr_capi.tune_table()] == [k]
     out, st = gpupr_capi.graph_cut(g["vertices"], tets, nbrs, g["labels"], g["fill_T"])

@@ -274,7 +274,7 @@ TuneEntry two_stage_tune(ReducedGraph& g, const Segments* segs, const gpupr_solv
     std::vector<TuneCand> c1;
     c1.push_back({0, 0.0, 0, 0, {}, {}});
     for (int bp : {1, 2, 3, 4})
-        for (double f : {0.5, 1.0, 2.0}) c1.push_back({bp, f, 0, 0, {}, {}});
+        for (double f : {0.25, 0.5, 1.0, 2.0}) c1.push_back({bp, f, 0, 0, {}, {}});
     run(c1);
     size_t bi = 1;
     for (size_t i = 2; i < c1.size(); ++i)
