@@ -647,7 +647,11 @@ def run_raw(args, local):
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    res = [gpupr_capi.solve_ell(*d) for d in dg]
+    res, call_ms = [], []
+    for d in dg:
+        t0 = time.perf_counter()
+        res.append(gpupr_capi.solve_ell(*d))
+        call_ms.append(1e3 * (time.perf_counter() - t0))
     b.record(stream)
     torch.cuda.synchronize()
     seq_ms = a.elapsed_time(b)
@@ -706,6 +710,8 @@ def run_raw(args, local):
             "seeds": len(dg), "nodes_per_seed": sizes[0], "nodes": total,
             "flows": [int(r[0]) for r in res], "every_cut_capacity_equals_flow": bool(certified),
             "sequential_ms": round(seq_ms, 3), "nodes_per_s": round(total / (seq_ms * 1e-3), 1),
+            "sequential_call_ms": [round(x, 2) for x in call_ms],
+            "sequential_solve_device_ms": [round(r[2]["solve_device_ms"], 2) for r in res],
             "union_ms": round(union_ms, 3), "union_nodes_per_s": round(total / (union_ms * 1e-3), 1),
             "union_identical_to_separate": bool(union_same),
             "seed0": {"ms": round(st0["solve_device_ms"], 3), "rounds": int(st0["rounds"]),
