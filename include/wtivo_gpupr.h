@@ -128,6 +128,9 @@ typedef struct {
                                      bfs_bottom_up_ratio x the frontier);
                                      0 = top-down only (default) */
     double bfs_bottom_up_ratio;   /* default 1 */
+    int32_t bfs_chain_hops;       /* persistent engine: nodes one thread may label
+                                     in a row in a BFS step over a short frontier
+                                     (1 = level by level; default 4) */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

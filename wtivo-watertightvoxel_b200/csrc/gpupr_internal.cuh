@@ -262,6 +262,7 @@ struct SolveOptions {
     int engine = 0;                // 0 auto, 1 one launch per step, 2 persistent
     int chain_hops = 0;            // persistent engine: 0 = default
     int chain_max_active = 0;      // persistent engine: 0 = default
+    int bfs_chain_hops = 0;        // persistent engine: 0 = default
     int bfs_bottom_up = 0;         // persistent engine: direction-optimizing relabels
     double bfs_bottom_up_ratio = 1.0;
     int max_blocks_per_sm = 0;     // persistent engine: cap on the grid (0 = none); the

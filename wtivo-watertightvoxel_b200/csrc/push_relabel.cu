@@ -1102,6 +1102,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
         r.engine = o->engine;
         if (o->chain_hops > 0) r.chain_hops = o->chain_hops;
         if (o->chain_max_active > 0) r.chain_max_active = o->chain_max_active;
+        if (o->bfs_chain_hops > 0) r.bfs_chain_hops = o->bfs_chain_hops;
         r.bfs_bottom_up = o->bfs_bottom_up;
         if (o->bfs_bottom_up_ratio > 0) r.bfs_bottom_up_ratio = o->bfs_bottom_up_ratio;
     }
@@ -1193,7 +1194,7 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     // slow any graph down (a 2.9M-node torus: 6.6 ms, 10.0 with 32768).  The
     // autotuner may pick another setting.
     gv.chain_hops = opt.chain_hops > 0 ? opt.chain_hops : tuned ? te.chain_hops : 4;
-    gv.bfs_hops = BFS_CHAIN_HOPS;
+    gv.bfs_hops = opt.bfs_chain_hops > 0 ? std::min(opt.bfs_chain_hops, 64) : BFS_CHAIN_HOPS;
     gv.chain_max_active = opt.chain_max_active > 0 ? (uint32_t)opt.chain_max_active
                           : tuned                  ? (uint32_t)te.chain_max_active
                           : g.n < 1500000u         ? 131072u

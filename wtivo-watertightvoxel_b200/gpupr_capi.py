@@ -58,6 +58,7 @@ class SolveOptions(ctypes.Structure):
         ("work_relabel_factor", ctypes.c_double), ("engine", ctypes.c_int32),
         ("chain_hops", ctypes.c_int32), ("chain_max_active", ctypes.c_int32),
         ("bfs_bottom_up", ctypes.c_int32), ("bfs_bottom_up_ratio", ctypes.c_double),
+        ("bfs_chain_hops", ctypes.c_int32),
     ]
 
 
