@@ -46,6 +46,7 @@ from __future__ import annotations
 
 import argparse
 import contextlib
+import gc
 import json
 import os
 import subprocess
@@ -231,6 +232,18 @@ def make_graph(n_tets, seed):
     import synth
 
     return synth.config2(seed, n_tets=int(n_tets))
+
+
+@contextlib.contextmanager
+def no_gc():
+    """A timed loop of many host calls without the Python collector's pauses
+    (the bench process holds many large objects by the later legs)."""
+    gc.collect()
+    gc.disable()
+    try:
+        yield
+    finally:
+        gc.enable()
 
 
 @contextlib.contextmanager
@@ -646,14 +659,15 @@ def run_raw(args, local):
         gpupr_capi.solve_ell(*d)
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    res, call_ms = [], []
-    for d in dg:
-        t0 = time.perf_counter()
-        res.append(gpupr_capi.solve_ell(*d))
-        call_ms.append(1e3 * (time.perf_counter() - t0))
-    b.record(stream)
-    torch.cuda.synchronize()
+    with no_gc():
+        a.record(stream)
+        res, call_ms = [], []
+        for d in dg:
+            t0 = time.perf_counter()
+            res.append(gpupr_capi.solve_ell(*d))
+            call_ms.append(1e3 * (time.perf_counter() - t0))
+        b.record(stream)
+        torch.cuda.synchronize()
     seq_ms = a.elapsed_time(b)
     certified = all(_cut_capacity(*d, r[1]) == r[0] for d, r in zip(dg, res))
     # the seeds as one disjoint-union graph
@@ -935,11 +949,12 @@ def run_batch(args, local):
         gpupr_capi.graph_cut_batch(toff, voff, v, t, nb, l, 10.0, out=out)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        a.record(stream)
-        for _ in range(reps):
-            _, items, bst = gpupr_capi.graph_cut_batch(toff, voff, v, t, nb, l, 10.0, out=out)
-        b.record(stream)
-        torch.cuda.synchronize()
+        with no_gc():
+            a.record(stream)
+            for _ in range(reps):
+                _, items, bst = gpupr_capi.graph_cut_batch(toff, voff, v, t, nb, l, 10.0, out=out)
+            b.record(stream)
+            torch.cuda.synchronize()
         return a.elapsed_time(b) / reps, items, bst
 
     old = gpupr_capi.batch_tune_table()
@@ -956,11 +971,12 @@ def run_batch(args, local):
             gpupr_capi.graph_cut(gv, gt, gn, gl, 10.0, out=o)
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        seq = [gpupr_capi.graph_cut(gv, gt, gn, gl, 10.0, out=o)[1]
-               for (gt, gn, gv, gl), o in zip(singles, outs)]
-        b.record(stream)
-        torch.cuda.synchronize()
+        with no_gc():
+            a.record(stream)
+            seq = [gpupr_capi.graph_cut(gv, gt, gn, gl, 10.0, out=o)[1]
+                   for (gt, gn, gv, gl), o in zip(singles, outs)]
+            b.record(stream)
+            torch.cuda.synchronize()
         seq_ms = a.elapsed_time(b)
         toff = packed[0]
         ob = out.cpu().numpy()
