@@ -324,7 +324,7 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     stats = []
-    with Clocks(local) as clk:
+    with Clocks(local) as clk, no_gc():
         barrier(world)
         torch.cuda.synchronize()
         e0.record(stream)
@@ -442,6 +442,8 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         serial_ms = a.elapsed_time(b) / args.steps
         barrier(world)
+        gc.collect()
+        gc.disable()
         a.record(cut_stream)
         upload(0)
         cut_wall, up_wall, join_wall = [], [], []
@@ -465,6 +467,7 @@ def run_ours(args, world, rank, local):
             join_wall.append(time.perf_counter() - t0)
         b.record(cut_stream)
         torch.cuda.synchronize()
+        gc.enable()
         ems, evalue = whole_job(N, a.elapsed_time(b) / args.steps, world)
         serial_ms = max_over_ranks(serial_ms, world)
         h2d = pt.numel() * 4 + pn.numel() * 4 + hV.nbytes + hL.nbytes
