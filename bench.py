@@ -378,7 +378,11 @@ def run_ours(args, world, rank, local):
                 "phase_ms_per_step": {"solve": round(sum(s["solve_device_ms"] for s in stats) / args.steps, 3),
                                       "build": round(sum(s["build_device_ms"] for s in stats) / args.steps, 3),
                                       "global_relabel": round(bfs_ms / args.steps, 3),
-                                      "discharge": round(dis_ms / args.steps, 3)}}
+                                      "discharge": round(dis_ms / args.steps, 3)},
+                "bfs_steps_by_frontier": {"le_1024": int(stats[-1]["bfs_steps_by_frontier"][0]),
+                                          "le_16384": int(stats[-1]["bfs_steps_by_frontier"][1]),
+                                          "larger": int(stats[-1]["bfs_steps_by_frontier"][2]),
+                                          "ms": [round(x, 3) for x in stats[-1]["bfs_ms_by_frontier"]]}}
     if rank == 0:
         rs = random_sector_rate(dev)
         roofline["random_sector_gbs"] = round(rs, 1)

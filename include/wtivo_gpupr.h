@@ -89,6 +89,9 @@ typedef struct {
     uint64_t graphs_retired;    /* batch: graphs finished and left out of the
                                    relabels before the last one */
     uint64_t bottom_up_steps;   /* BFS steps run bottom-up (bfs_bottom_up) */
+    uint64_t bfs_steps_by_frontier[3];  /* persistent engine: BFS steps over frontiers
+                                           of <= 1024, <= 16384 and more nodes */
+    double bfs_ms_by_frontier[3];       /* ... and their time (block 0's clock) */
 } gpupr_cut_stats;
 
 /* Solver tuning knobs; zero fields take the defaults shown. */

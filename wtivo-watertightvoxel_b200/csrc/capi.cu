@@ -218,6 +218,10 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
     st->sweep_ms = sr.sweep_ms;
     st->graphs_retired = sr.graphs_retired;
     st->bottom_up_steps = sr.bottom_up_steps;
+    for (int k = 0; k < 3; ++k) {
+        st->bfs_steps_by_frontier[k] = sr.step_cnt[k];
+        st->bfs_ms_by_frontier[k] = sr.step_ms[k];
+    }
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -539,6 +543,10 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     st->sweep_ms = sr.sweep_ms;
     st->graphs_retired = sr.graphs_retired;
     st->bottom_up_steps = sr.bottom_up_steps;
+    for (int k = 0; k < 3; ++k) {
+        st->bfs_steps_by_frontier[k] = sr.step_cnt[k];
+        st->bfs_ms_by_frontier[k] = sr.step_ms[k];
+    }
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -782,6 +790,10 @@ gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_r
             stats->sweep_ms = sr.sweep_ms;
             stats->graphs_retired = sr.graphs_retired;
             stats->bottom_up_steps = sr.bottom_up_steps;
+            for (int k = 0; k < 3; ++k) {
+                stats->bfs_steps_by_frontier[k] = sr.step_cnt[k];
+                stats->bfs_ms_by_frontier[k] = sr.step_ms[k];
+            }
             stats->kernel_launches = launches;
         }
     });
@@ -847,6 +859,10 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
             stats->sweep_ms = sr.sweep_ms;
             stats->graphs_retired = sr.graphs_retired;
             stats->bottom_up_steps = sr.bottom_up_steps;
+            for (int k = 0; k < 3; ++k) {
+                stats->bfs_steps_by_frontier[k] = sr.step_cnt[k];
+                stats->bfs_ms_by_frontier[k] = sr.step_ms[k];
+            }
             stats->kernel_launches = launches;
         }
     });

@@ -54,6 +54,11 @@ struct Ctl {
     uint32_t lab_cnt[3];
     uint32_t bu_cnt[3];
     uint32_t bu_steps;
+    // persistent engine: BFS steps by frontier size (<= 1024, <= 16384,
+    // larger) and block 0's time in each class
+    uint32_t step_cnt[3];
+    uint32_t pad3;
+    unsigned long long step_ns[3];
 };
 
 // Nodes per pass of a whole-array sweep (seed, excess init, active sweep):
@@ -305,6 +310,8 @@ struct SolveResult {
     uint64_t workspace_bytes = 0;
     uint64_t graphs_retired = 0;   // segmented solves: graphs finished before the last relabel
     uint64_t bottom_up_steps = 0;  // BFS steps run bottom-up
+    uint64_t step_cnt[3] = {0, 0, 0};  // BFS steps by frontier size (<= 1024, <= 16384, larger)
+    double step_ms[3] = {0, 0, 0};
     int engine = 1;                // 1 one launch per step, 2 persistent
     int blocks_per_sm = 0;         // persistent engine: grid used
     double work_factor = 0.0;      // persistent engine: relabel work factor used

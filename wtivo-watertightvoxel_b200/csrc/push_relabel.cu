@@ -858,6 +858,8 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
     // s_clk = {BFS, active sweep, discharge, last mark} (shared memory, so it
     // holds no registers through the solve)
     __shared__ unsigned long long s_clk[4];
+    __shared__ unsigned long long s_step_ns[3];
+    __shared__ uint32_t s_step_cnt[3];
     auto lap = [&](int phase) {
         if (lead) {
             const unsigned long long t = gtimer();
@@ -883,7 +885,11 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
         unsigned long long rounds_total = 0;
         uint32_t levels_total = 0, relabels = 0;
         bool ok = true;
-        if (lead) { s_clk[0] = s_clk[1] = s_clk[2] = 0ull; s_clk[3] = gtimer(); }
+        if (lead) {
+            s_clk[0] = s_clk[1] = s_clk[2] = 0ull;
+            s_clk[3] = gtimer();
+            for (int k = 0; k < 3; ++k) { s_step_ns[k] = 0ull; s_step_cnt[k] = 0u; }
+        }
         while (ok) {
             // ---- global relabel (label-correcting steps, reachability exact) ----
             bfs_seed_body<false>(g, s_buf, s_buf + DTPB * 4, s_m);
@@ -896,6 +902,7 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
                 const uint32_t cnt = min(vload(&ctl->bfs_cnt[L % 3]), g.n);
                 if (cnt == 0) break;
                 if (lead) ctl->bfs_cnt[(L + 2) % 3] = 0u;
+                const unsigned long long t_step = lead ? gtimer() : 0ull;
                 // every decision below is the same in every block: it depends
                 // on counters completed before the last barrier
                 bool bottom_up = false;
@@ -922,6 +929,11 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
                     if (hops > 1) exact = false;
                 }
                 if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
+                if (lead) {
+                    const int c = cnt <= 1024u ? 0 : (cnt <= 16384u ? 1 : 2);
+                    s_step_ns[c] += gtimer() - t_step;
+                    ++s_step_cnt[c];
+                }
                 ++L;
                 ++levels_total;
                 if (L > g.n + 2u) {   // a BFS labels a new node per level
@@ -987,6 +999,10 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
             ctl->rounds_done = (uint32_t)rounds_total;
             ctl->bfs_levels = levels_total;
             ctl->relabel_phases = relabels;
+            for (int k = 0; k < 3; ++k) {
+                ctl->step_cnt[k] = s_step_cnt[k];
+                ctl->step_ns[k] = s_step_ns[k];
+            }
             ctl->bfs_ns = s_clk[0];
             ctl->sweep_ns = s_clk[1];
             ctl->discharge_ns = s_clk[2];
@@ -1237,6 +1253,10 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     out.sweep_ms = (double)hc.sweep_ns * 1e-6;
     out.graphs_retired = hc.segs_retired;
     out.bottom_up_steps = hc.bu_steps;
+    for (int k = 0; k < 3; ++k) {
+        out.step_cnt[k] = hc.step_cnt[k];
+        out.step_ms[k] = (double)hc.step_ns[k] * 1e-6;
+    }
     out.solve_s = std::chrono::duration<double>(Clock::now() - t0).count();
 }
 

@@ -39,6 +39,7 @@ STATS_FIELDS = [
     ("chain_hops", ctypes.c_int64), ("chain_max_active", ctypes.c_int64),
     ("sweep_ms", ctypes.c_double), ("graphs_retired", ctypes.c_uint64),
     ("bottom_up_steps", ctypes.c_uint64),
+    ("bfs_steps_by_frontier", ctypes.c_uint64 * 3), ("bfs_ms_by_frontier", ctypes.c_double * 3),
 ]
 
 
@@ -46,7 +47,8 @@ class CutStats(ctypes.Structure):
     _fields_ = STATS_FIELDS
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        return {k: (list(v) if isinstance(v, ctypes.Array) else v)
+                for k, v in ((k, getattr(self, k)) for k, _ in self._fields_)}
 
 
 class SolveOptions(ctypes.Structure):
