@@ -92,6 +92,8 @@ typedef struct {
     uint64_t bfs_steps_by_frontier[3];  /* persistent engine: BFS steps over frontiers
                                            of <= 1024, <= 16384 and more nodes */
     double bfs_ms_by_frontier[3];       /* ... and their time (block 0's clock) */
+    uint64_t bfs_tail_steps;    /* BFS steps run by one block (bfs_tail_max) */
+    uint64_t bfs_tail_levels;   /* ... and the levels they covered */
 } gpupr_cut_stats;
 
 /* Solver tuning knobs; zero fields take the defaults shown. */
@@ -134,6 +136,10 @@ typedef struct {
     int32_t bfs_chain_hops;       /* persistent engine: nodes one thread may label
                                      in a row in a BFS step over a short frontier
                                      (1 = level by level; default 4) */
+    int32_t bfs_tail_max;         /* persistent engine: a BFS frontier of at most
+                                     this many nodes (up to 1024) is expanded by
+                                     one block alone, level after level, with
+                                     block-level syncs (0 = default, < 0 = never) */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

@@ -222,6 +222,8 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
         st->bfs_steps_by_frontier[k] = sr.step_cnt[k];
         st->bfs_ms_by_frontier[k] = sr.step_ms[k];
     }
+    st->bfs_tail_steps = sr.tail_steps;
+    st->bfs_tail_levels = sr.tail_levels;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -547,6 +549,8 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
         st->bfs_steps_by_frontier[k] = sr.step_cnt[k];
         st->bfs_ms_by_frontier[k] = sr.step_ms[k];
     }
+    st->bfs_tail_steps = sr.tail_steps;
+    st->bfs_tail_levels = sr.tail_levels;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -794,6 +798,8 @@ gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_r
                 stats->bfs_steps_by_frontier[k] = sr.step_cnt[k];
                 stats->bfs_ms_by_frontier[k] = sr.step_ms[k];
             }
+            stats->bfs_tail_steps = sr.tail_steps;
+            stats->bfs_tail_levels = sr.tail_levels;
             stats->kernel_launches = launches;
         }
     });
@@ -863,6 +869,8 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
                 stats->bfs_steps_by_frontier[k] = sr.step_cnt[k];
                 stats->bfs_ms_by_frontier[k] = sr.step_ms[k];
             }
+            stats->bfs_tail_steps = sr.tail_steps;
+            stats->bfs_tail_levels = sr.tail_levels;
             stats->kernel_launches = launches;
         }
     });

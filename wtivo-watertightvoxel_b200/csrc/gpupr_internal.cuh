@@ -57,8 +57,10 @@ struct Ctl {
     // persistent engine: BFS steps by frontier size (<= 1024, <= 16384,
     // larger) and block 0's time in each class
     uint32_t step_cnt[3];
-    uint32_t pad3;
+    uint32_t tail_L;         // persistent engine: BFS level after a tail step of block 0
     unsigned long long step_ns[3];
+    unsigned long long tail_steps;   // tail steps and the levels they covered
+    unsigned long long tail_levels;
 };
 
 // Nodes per pass of a whole-array sweep (seed, excess init, active sweep):
@@ -107,6 +109,9 @@ struct SolveView {
     uint32_t* cand[2];
     int bottom_up;
     float bu_ratio;
+    uint32_t tail_max;                  // persistent engine: frontiers up to this size are
+                                        // expanded by block 0 alone, level after level
+                                        // (0: never)
 };
 
 // ---------------------------------------------------------------------------
@@ -268,6 +273,7 @@ struct SolveOptions {
     int chain_hops = 0;            // persistent engine: 0 = default
     int chain_max_active = 0;      // persistent engine: 0 = default
     int bfs_chain_hops = 0;        // persistent engine: 0 = default
+    int bfs_tail_max = 0;          // persistent engine: 0 = default, < 0 = never
     int bfs_bottom_up = 0;         // persistent engine: direction-optimizing relabels
     double bfs_bottom_up_ratio = 1.0;
     int max_blocks_per_sm = 0;     // persistent engine: cap on the grid (0 = none); the
@@ -310,6 +316,7 @@ struct SolveResult {
     uint64_t workspace_bytes = 0;
     uint64_t graphs_retired = 0;   // segmented solves: graphs finished before the last relabel
     uint64_t bottom_up_steps = 0;  // BFS steps run bottom-up
+    uint64_t tail_steps = 0, tail_levels = 0;   // BFS tail steps of block 0, levels covered
     uint64_t step_cnt[3] = {0, 0, 0};  // BFS steps by frontier size (<= 1024, <= 16384, larger)
     double step_ms[3] = {0, 0, 0};
     int engine = 1;                // 1 one launch per step, 2 persistent

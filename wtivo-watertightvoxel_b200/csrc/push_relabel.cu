@@ -524,6 +524,90 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
     }
 }
 
+// Frontier entries block 0 keeps in shared memory in a tail step, and the
+// most levels one tail step covers (a bound on the other blocks' barrier wait).
+constexpr uint32_t TAIL_CAP = DTPB * 4u;
+constexpr int TAIL_LEVELS = 4096;
+// Default frontier size up to which tail steps run (0: none).
+constexpr uint32_t BFS_TAIL_DEFAULT = 0u;
+
+// A tail step of the persistent engine's BFS, run by block 0 alone while the
+// other blocks wait at the grid barrier: starting from level L0's frontier
+// (cnt0 <= TAIL_CAP nodes), it expands level after level with the frontier in
+// shared memory and block-level syncs instead of a grid barrier per level
+// (the same label-correcting rule as bfs_step_body: a neighbour with an arc
+// into u and a label above h(u)+1 is lowered by atomicMin and queued when
+// first labelled, or when improved while 4 x frontier <= n).  It stops when a
+// frontier is empty, no longer fits in shared memory or exceeds g.tail_max,
+// or after TAIL_LEVELS levels; it then leaves that level's frontier in the
+// global queue for it with its count, every other ring counter at zero, and
+// the level in ctl->tail_L.  s_buf holds 2 * TAIL_CAP entries; s_m[10] is the
+// claim counter.
+__device__ void bfs_tail_body(const SolveView& g, uint32_t L0, uint32_t cnt0, uint32_t* s_buf,
+                              uint32_t* s_m, unsigned long long& visits)
+{
+    Ctl* ctl = g.ctl;
+    uint32_t* sA = s_buf;
+    uint32_t* sB = s_buf + TAIL_CAP;
+    const uint32_t* in0 = (L0 & 1) ? g.fr[1] : g.fr[0];
+    for (uint32_t i = threadIdx.x; i < cnt0; i += DTPB) sA[i] = __ldcg(in0 + i);
+    uint32_t L = L0, nA = cnt0;
+    __syncthreads();
+    for (int lv = 0;; ++lv) {
+        // expand level L (frontier sA[0..nA)) into level L+1
+        uint32_t* out = (L & 1) ? g.fr[0] : g.fr[1];   // level L+1's global queue
+        const bool propagate = 4ull * nA <= (unsigned long long)g.n;
+        if (threadIdx.x == 0) s_m[10] = 0u;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < nA; i += DTPB) {
+            const uint32_t u = sA[i];
+            const uint32_t hu = ldcg(g.height + u);
+            if (hu >= g.n) continue;
+            uint32_t arcs;
+            const int4 nb4 = residual_in_arcs(g, u, &arcs);
+            const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+            const uint32_t cand = hu + 1u;
+            ++visits;
+            uint32_t hv[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) hv[k] = ((arcs >> k) & 1u) ? ldcg(g.height + nb[k]) : 0u;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int v = nb[k];
+                if (!((arcs >> k) & 1u) || hv[k] <= cand) continue;
+                const uint32_t old = atomicMin(g.height + v, cand);
+                if (old <= cand || (old != UNVIS && !propagate)) continue;
+                // entries past the shared array go straight to the global queue,
+                // behind room for the shared ones
+                const uint32_t idx = atomicAdd(&s_m[10], 1u);
+                if (idx < TAIL_CAP) sB[idx] = (uint32_t)v;
+                else if (idx < g.n) out[idx] = (uint32_t)v;
+                else raise_error(ctl, (int)GPUPR_ERR_INVARIANT);
+            }
+        }
+        __syncthreads();
+        const uint32_t nB = min(s_m[10], g.n);
+        ++L;
+        if (nB == 0u || nB > TAIL_CAP || nB > g.tail_max || lv + 1 >= TAIL_LEVELS || L > g.n + 2u) {
+            const uint32_t m = min(nB, TAIL_CAP);
+            for (uint32_t i = threadIdx.x; i < m; i += DTPB) out[i] = sB[i];
+            if (threadIdx.x == 0) {
+                for (int k = 0; k < 3; ++k) ctl->bfs_cnt[k] = 0u;
+                ctl->bfs_cnt[L % 3] = nB;
+                ctl->tail_L = L;
+                ctl->tail_steps += 1ull;
+                ctl->tail_levels += (unsigned long long)(L - L0);
+            }
+            return;
+        }
+        uint32_t* t = sA;
+        sA = sB;
+        sB = t;
+        nA = nB;
+        __syncthreads();
+    }
+}
+
 // One bottom-up step j of a direction-optimizing relabel (frontier label L):
 // every candidate v of list j (cand[j % 2], size in bu_cnt[j % 3]; list 0 is
 // the previous relabel's reached set, which holds every node this relabel can
@@ -825,6 +909,9 @@ __device__ bool grid_barrier(Ctl* ctl, unsigned long long& target, unsigned long
             const unsigned long long v = ld_acquire(&ctl->bar);
             if (v & BAR_ABORT) { ok = 0; break; }
             if ((v & BAR_COUNT) >= target) break;
+            // a long wait (block 0's BFS tail) polls less often, off the L2
+            // slice that holds the counter
+            if (it >= 2048u) __nanosleep(256);
             if ((it & 63u) == 0u) {
                 const unsigned long long t = gtimer();
                 if (it == 0u) t0 = t;
@@ -912,6 +999,25 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
                     const uint32_t cc = vload(&ctl->cand_cnt);
                     const uint32_t rem = cc > labelled ? cc - labelled : 0u;
                     bottom_up = cc != 0u && (float)rem <= g.bu_ratio * (float)cnt;
+                }
+                if (!g.bottom_up && g.tail_max && cnt <= g.tail_max) {
+                    // a short frontier: block 0 runs the next levels alone
+                    if (blockIdx.x == 0) bfs_tail_body(g, L, cnt, s_buf, s_m, bfs_visits);
+                    exact = false;
+                    if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
+                    if (lead) {
+                        s_step_ns[0] += gtimer() - t_step;
+                        ++s_step_cnt[0];
+                    }
+                    const uint32_t Lt = vload(&ctl->tail_L);
+                    levels_total += Lt - L;
+                    L = Lt;
+                    if (L > g.n + 2u) {
+                        if (lead) raise_error(ctl, (int)GPUPR_ERR_INVARIANT);
+                        ok = false;
+                        break;
+                    }
+                    continue;
                 }
                 if (bottom_up) {
                     bfs_bottom_up_body(g, L, bu_j, s_buf, s_buf + DTPB * 4, DTPB * 4, s_m, bfs_visits);
@@ -1119,6 +1225,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
         if (o->chain_hops > 0) r.chain_hops = o->chain_hops;
         if (o->chain_max_active > 0) r.chain_max_active = o->chain_max_active;
         if (o->bfs_chain_hops > 0) r.bfs_chain_hops = o->bfs_chain_hops;
+        r.bfs_tail_max = o->bfs_tail_max;
         r.bfs_bottom_up = o->bfs_bottom_up;
         if (o->bfs_bottom_up_ratio > 0) r.bfs_bottom_up_ratio = o->bfs_bottom_up_ratio;
     }
@@ -1211,6 +1318,9 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     // autotuner may pick another setting.
     gv.chain_hops = opt.chain_hops > 0 ? opt.chain_hops : tuned ? te.chain_hops : 4;
     gv.bfs_hops = opt.bfs_chain_hops > 0 ? std::min(opt.bfs_chain_hops, 64) : BFS_CHAIN_HOPS;
+    gv.tail_max = opt.bfs_tail_max < 0 ? 0u
+                  : opt.bfs_tail_max > 0 ? std::min<uint32_t>((uint32_t)opt.bfs_tail_max, TAIL_CAP)
+                                         : BFS_TAIL_DEFAULT;
     gv.chain_max_active = opt.chain_max_active > 0 ? (uint32_t)opt.chain_max_active
                           : tuned                  ? (uint32_t)te.chain_max_active
                           : g.n < 1500000u         ? 131072u
@@ -1253,6 +1363,8 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     out.sweep_ms = (double)hc.sweep_ns * 1e-6;
     out.graphs_retired = hc.segs_retired;
     out.bottom_up_steps = hc.bu_steps;
+    out.tail_steps = hc.tail_steps;
+    out.tail_levels = hc.tail_levels;
     for (int k = 0; k < 3; ++k) {
         out.step_cnt[k] = hc.step_cnt[k];
         out.step_ms[k] = (double)hc.step_ns[k] * 1e-6;

@@ -40,6 +40,7 @@ STATS_FIELDS = [
     ("sweep_ms", ctypes.c_double), ("graphs_retired", ctypes.c_uint64),
     ("bottom_up_steps", ctypes.c_uint64),
     ("bfs_steps_by_frontier", ctypes.c_uint64 * 3), ("bfs_ms_by_frontier", ctypes.c_double * 3),
+    ("bfs_tail_steps", ctypes.c_uint64), ("bfs_tail_levels", ctypes.c_uint64),
 ]
 
 
@@ -60,7 +61,7 @@ class SolveOptions(ctypes.Structure):
         ("work_relabel_factor", ctypes.c_double), ("engine", ctypes.c_int32),
         ("chain_hops", ctypes.c_int32), ("chain_max_active", ctypes.c_int32),
         ("bfs_bottom_up", ctypes.c_int32), ("bfs_bottom_up_ratio", ctypes.c_double),
-        ("bfs_chain_hops", ctypes.c_int32),
+        ("bfs_chain_hops", ctypes.c_int32), ("bfs_tail_max", ctypes.c_int32),
     ]
 
 
