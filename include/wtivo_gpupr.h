@@ -140,6 +140,9 @@ typedef struct {
                                      this many nodes (up to 1024) is expanded by
                                      one block alone, level after level, with
                                      block-level syncs (0 = default, < 0 = never) */
+    int32_t discharge_warp_aggregate; /* persistent engine: 1 = lanes of a warp that
+                                     push to the same neighbour add their amounts
+                                     with one atomic (default 0: one atomic each) */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

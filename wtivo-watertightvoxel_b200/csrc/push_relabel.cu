@@ -47,7 +47,12 @@
 #include <cmath>
 #include <string>
 
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
 #include "gpupr_internal.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace gpupr {
 namespace {
@@ -672,6 +677,7 @@ __device__ __forceinline__ void bfs_bottom_up_body(const SolveView& g, uint32_t 
 // whose excess this discharge moved from 0 up is owned by this thread, and
 // instead of queueing it for the next round the thread may carry on with
 // it, so excess can travel several hops per round), or UNVIS.
+template <bool kAgg>
 __device__ __forceinline__ uint32_t discharge_node(const SolveView& g, uint32_t v, const Stage& st,
                                                    bool may_chain, Work& w)
 {
@@ -727,9 +733,22 @@ __device__ __forceinline__ uint32_t discharge_node(const SolveView& g, uint32_t 
             const uint32_t rk = (rv >> (2 * best)) & 3u;
             atomicSub(g.res + (size_t)v * 4u + best, d);
             atomicAdd(g.res + (size_t)u * 4u + rk, d);
-            const unsigned long long old =
-                atomicAdd(reinterpret_cast<unsigned long long*>(g.excess + u), (unsigned long long)d);
-            if (old == 0ull) {
+            bool owner;
+            if (kAgg) {
+                // lanes pushing to the same neighbour now add their amounts in
+                // one atomic, issued by the group's first lane, which takes
+                // ownership when the neighbour's excess was zero
+                const cg::coalesced_group active = cg::coalesced_threads();
+                const cg::coalesced_group same = cg::labeled_partition(active, (unsigned)u);
+                const unsigned long long sum = cg::reduce(same, (unsigned long long)d,
+                                                          cg::plus<unsigned long long>());
+                owner = same.thread_rank() == 0 &&
+                        atomicAdd(reinterpret_cast<unsigned long long*>(g.excess + u), sum) == 0ull;
+            } else {
+                owner = atomicAdd(reinterpret_cast<unsigned long long*>(g.excess + u),
+                                  (unsigned long long)d) == 0ull;
+            }
+            if (owner) {
                 if (may_chain && next == UNVIS) next = (uint32_t)u;
                 else stage_push(g, st, (uint32_t)u);
             }
@@ -760,6 +779,7 @@ __device__ __forceinline__ uint32_t discharge_node(const SolveView& g, uint32_t 
 // One discharge round over cnt active nodes: discharge each, stage the nodes
 // that become (or stay) active, append them to the next active queue.
 // `first` is the thread's first entry (prefetch_entry).
+template <bool kAgg>
 __device__ __forceinline__ void discharge_body(const SolveView& g, uint32_t round, uint32_t cnt,
                                                uint32_t first, uint32_t* s_buf, uint32_t stage_cap,
                                                uint32_t* s_m, Work& w)
@@ -776,7 +796,7 @@ __device__ __forceinline__ void discharge_body(const SolveView& g, uint32_t roun
             uint32_t v = (it == 0 && cnt <= SPREAD_MAX) ? first : __ldcg(in + i);
             if (v < g.n) {
                 for (int hop = 1;; ++hop) {
-                    v = discharge_node(g, v, st, hop < hops, w);
+                    v = discharge_node<kAgg>(g, v, st, hop < hops, w);
                     if (v == UNVIS) break;
                 }
             } else {
@@ -827,7 +847,7 @@ __global__ void __launch_bounds__(DTPB) k_discharge(SolveView g, uint32_t round)
     Work w;
     if (threadIdx.x == 0) s_m[0] = 0;
     __syncthreads();
-    discharge_body(g, round, cnt, first, s_buf, DTPB * 5, s_m, w);
+    discharge_body<false>(g, round, cnt, first, s_buf, DTPB * 5, s_m, w);
     reduce_work(ctl, w, 0ull, s_red);
 }
 
@@ -928,6 +948,8 @@ __device__ bool grid_barrier(Ctl* ctl, unsigned long long& target, unsigned long
     return *s_ok != 0;
 }
 
+// kAgg: warp-aggregated excess atomics in the discharge (an option).
+template <bool kAgg>
 __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, PersistParams p)
 {
     __shared__ uint32_t s_buf[DTPB * 8];
@@ -1070,7 +1092,7 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
                     break;
                 }
                 if (lead) ctl->act_cnt[(r + 2) % 3] = 0u;
-                discharge_body(g, r, cnt, first, s_buf, DTPB * 8, s_m, w);
+                discharge_body<kAgg>(g, r, cnt, first, s_buf, DTPB * 8, s_m, w);
                 if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
                 ++r;
                 ++rounds_total;
@@ -1226,6 +1248,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
         if (o->chain_max_active > 0) r.chain_max_active = o->chain_max_active;
         if (o->bfs_chain_hops > 0) r.bfs_chain_hops = o->bfs_chain_hops;
         r.bfs_tail_max = o->bfs_tail_max;
+        r.discharge_warp_aggregate = o->discharge_warp_aggregate;
         r.bfs_bottom_up = o->bfs_bottom_up;
         if (o->bfs_bottom_up_ratio > 0) r.bfs_bottom_up_ratio = o->bfs_bottom_up_ratio;
     }
@@ -1244,7 +1267,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
 int persistent_blocks_per_sm()
 {
     int bps = 0;
-    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent, DTPB, 0));
+    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent<false>, DTPB, 0));
     return bps;
 }
 
@@ -1265,7 +1288,7 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
 {
     using Clock = std::chrono::steady_clock;
     int bps = 0;
-    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent, DTPB, 0));
+    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent<false>, DTPB, 0));
     if (bps < 1) throw Error{GPUPR_ERR_CUDA, "persistent solver kernel cannot be resident"};
     // resident blocks per SM: a step of a small graph is one chain of
     // dependent L2 round trips plus a grid barrier whose cost grows with the
@@ -1318,6 +1341,7 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     // autotuner may pick another setting.
     gv.chain_hops = opt.chain_hops > 0 ? opt.chain_hops : tuned ? te.chain_hops : 4;
     gv.bfs_hops = opt.bfs_chain_hops > 0 ? std::min(opt.bfs_chain_hops, 64) : BFS_CHAIN_HOPS;
+    gv.warp_agg = opt.discharge_warp_aggregate > 0 ? 1 : 0;
     gv.tail_max = opt.bfs_tail_max < 0 ? 0u
                   : opt.bfs_tail_max > 0 ? std::min<uint32_t>((uint32_t)opt.bfs_tail_max, TAIL_CAP)
                                          : BFS_TAIL_DEFAULT;
@@ -1327,8 +1351,9 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
                           : g.n < 2000000u         ? 32768u
                                                    : 4096u;
     void* args[] = {&gv, &p};
-    GPUPR_CUDA(cudaLaunchCooperativeKernel((const void*)k_solve_persistent, dim3(grid), dim3(DTPB),
-                                           args, 0, s));
+    const void* kern = gv.warp_agg ? (const void*)k_solve_persistent<true>
+                                   : (const void*)k_solve_persistent<false>;
+    GPUPR_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(DTPB), args, 0, s));
     GPUPR_CUDA(cudaEventRecord(e1, s));
     GPUPR_CUDA(cudaMemcpyAsync(pc, g.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaStreamSynchronize(s));
