@@ -143,6 +143,9 @@ typedef struct {
     int32_t discharge_warp_aggregate; /* persistent engine: 1 = lanes of a warp that
                                      push to the same neighbour add their amounts
                                      with one atomic (default 0: one atomic each) */
+    int32_t bfs_chain_max_frontier; /* persistent engine: BFS steps chain
+                                     (bfs_chain_hops) only over frontiers of at
+                                     most this many nodes (default 65536) */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

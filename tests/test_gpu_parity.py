@@ -101,6 +101,8 @@ def test_solver_invariants(built, kind, seed, size):
                                  dict(bfs_chain_hops=1), dict(bfs_chain_hops=16),
                                  dict(bfs_tail_max=1024), dict(bfs_tail_max=8, blocks_per_sm=1),
                                  dict(discharge_warp_aggregate=1),
+                                 dict(bfs_chain_max_frontier=1 << 30),
+                                 dict(bfs_chain_max_frontier=1 << 30, bfs_chain_hops=8),
                                  dict(discharge_warp_aggregate=1, chain_hops=1, local_steps=32),
                                  dict(bfs_tail_max=1024, bfs_chain_hops=1, work_relabel_factor=0.05),
                                  dict(bfs_bottom_up=1), dict(bfs_bottom_up=1, bfs_bottom_up_ratio=64.0),

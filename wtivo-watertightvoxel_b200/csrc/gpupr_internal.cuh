@@ -109,6 +109,7 @@ struct SolveView {
     uint32_t* cand[2];
     int bottom_up;
     float bu_ratio;
+    uint32_t bfs_chain_max;             // BFS steps chain (bfs_hops) over frontiers up to this size
     int warp_agg;                       // discharge: lanes pushing to the same neighbour
                                         // share one excess atomic
     uint32_t tail_max;                  // persistent engine: frontiers up to this size are
@@ -277,6 +278,7 @@ struct SolveOptions {
     int bfs_chain_hops = 0;        // persistent engine: 0 = default
     int bfs_tail_max = 0;          // persistent engine: 0 = default, < 0 = never
     int discharge_warp_aggregate = 0;   // persistent engine: 1 = warp-aggregated excess atomics
+    int bfs_chain_max_frontier = 0;     // persistent engine: 0 = default (65536)
     int bfs_bottom_up = 0;         // persistent engine: direction-optimizing relabels
     double bfs_bottom_up_ratio = 1.0;
     int max_blocks_per_sm = 0;     // persistent engine: cap on the grid (0 = none); the

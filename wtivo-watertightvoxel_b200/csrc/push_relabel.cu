@@ -1048,7 +1048,7 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
                     if (lead) ++ctl->bu_steps;
                 } else {
                     const unsigned long long nn = g.n;
-                    const int hops = (g.bfs_hops > 1 && cnt <= SPREAD_MAX &&
+                    const int hops = (g.bfs_hops > 1 && cnt <= g.bfs_chain_max &&
                                       4ull * (unsigned long long)g.bfs_hops * cnt <= nn)
                                          ? g.bfs_hops : 1;
                     const bool propagate = 4ull * (unsigned long long)hops * cnt <= nn;
@@ -1249,6 +1249,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
         if (o->bfs_chain_hops > 0) r.bfs_chain_hops = o->bfs_chain_hops;
         r.bfs_tail_max = o->bfs_tail_max;
         r.discharge_warp_aggregate = o->discharge_warp_aggregate;
+        if (o->bfs_chain_max_frontier > 0) r.bfs_chain_max_frontier = o->bfs_chain_max_frontier;
         r.bfs_bottom_up = o->bfs_bottom_up;
         if (o->bfs_bottom_up_ratio > 0) r.bfs_bottom_up_ratio = o->bfs_bottom_up_ratio;
     }
@@ -1342,6 +1343,7 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     gv.chain_hops = opt.chain_hops > 0 ? opt.chain_hops : tuned ? te.chain_hops : 4;
     gv.bfs_hops = opt.bfs_chain_hops > 0 ? std::min(opt.bfs_chain_hops, 64) : BFS_CHAIN_HOPS;
     gv.warp_agg = opt.discharge_warp_aggregate > 0 ? 1 : 0;
+    gv.bfs_chain_max = opt.bfs_chain_max_frontier > 0 ? (uint32_t)opt.bfs_chain_max_frontier : SPREAD_MAX;
     gv.tail_max = opt.bfs_tail_max < 0 ? 0u
                   : opt.bfs_tail_max > 0 ? std::min<uint32_t>((uint32_t)opt.bfs_tail_max, TAIL_CAP)
                                          : BFS_TAIL_DEFAULT;

@@ -62,7 +62,7 @@ class SolveOptions(ctypes.Structure):
         ("chain_hops", ctypes.c_int32), ("chain_max_active", ctypes.c_int32),
         ("bfs_bottom_up", ctypes.c_int32), ("bfs_bottom_up_ratio", ctypes.c_double),
         ("bfs_chain_hops", ctypes.c_int32), ("bfs_tail_max", ctypes.c_int32),
-        ("discharge_warp_aggregate", ctypes.c_int32),
+        ("discharge_warp_aggregate", ctypes.c_int32), ("bfs_chain_max_frontier", ctypes.c_int32),
     ]
 
 
