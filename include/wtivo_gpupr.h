@@ -145,7 +145,8 @@ typedef struct {
                                      with one atomic (default 0: one atomic each) */
     int32_t bfs_chain_max_frontier; /* persistent engine: BFS steps chain
                                      (bfs_chain_hops) only over frontiers of at
-                                     most this many nodes (default 65536) */
+                                     most this many nodes (default: any frontier
+                                     whose chained step fits the queue bound) */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

@@ -278,7 +278,7 @@ struct SolveOptions {
     int bfs_chain_hops = 0;        // persistent engine: 0 = default
     int bfs_tail_max = 0;          // persistent engine: 0 = default, < 0 = never
     int discharge_warp_aggregate = 0;   // persistent engine: 1 = warp-aggregated excess atomics
-    int bfs_chain_max_frontier = 0;     // persistent engine: 0 = default (65536)
+    int bfs_chain_max_frontier = 0;     // persistent engine: 0 = default (no limit)
     int bfs_bottom_up = 0;         // persistent engine: direction-optimizing relabels
     double bfs_bottom_up_ratio = 1.0;
     int max_blocks_per_sm = 0;     // persistent engine: cap on the grid (0 = none); the

