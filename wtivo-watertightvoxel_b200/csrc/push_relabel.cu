@@ -486,9 +486,9 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
         if (i < cnt) {
             uint32_t u = (it == 0 && cnt <= SPREAD_MAX) ? first : __ldcg(in + i);
             uint32_t hu = exact ? L : ldcg(g.height + u);
+            uint32_t arcs;
+            int4 nb4 = residual_in_arcs(g, u, &arcs);
             for (int hop = 1; hu < g.n; ++hop) {   // a queued node is labelled (< n)
-                uint32_t arcs;
-                const int4 nb4 = residual_in_arcs(g, u, &arcs);
                 const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
                 const uint32_t cand = hu + 1u;
                 uint32_t next = UNVIS;
@@ -498,6 +498,15 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
                 uint32_t hv[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) hv[k] = ((arcs >> k) & 1u) ? ldcg(g.height + nb[k]) : 0u;
+                // the chain's next node is normally the first neighbour that
+                // passes the label test: its in-arc row is loaded together
+                // with the label atomics, not after them
+                int pre_v = -1;
+#pragma unroll
+                for (int k = 3; k >= 0; --k)
+                    if (((arcs >> k) & 1u) && hv[k] > cand) pre_v = nb[k];
+                int4 pre = make_int4(-1, -1, -1, -1);
+                if (g.inrow && hop < hops && pre_v >= 0) pre = __ldcg(g.inrow + pre_v);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int v = nb[k];
@@ -511,6 +520,13 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
                 if (next == UNVIS) break;
                 u = next;
                 hu = cand;
+                if (g.inrow && (int)next == pre_v) {
+                    nb4 = pre;
+                    arcs = (uint32_t)(pre.x >= 0) | ((uint32_t)(pre.y >= 0) << 1) |
+                           ((uint32_t)(pre.z >= 0) << 2) | ((uint32_t)(pre.w >= 0) << 3);
+                } else {
+                    nb4 = residual_in_arcs(g, u, &arcs);
+                }
             }
         }
         __syncthreads();
