@@ -20,11 +20,13 @@
 extern "C" {
 #endif
 
-#define GPUPR_ABI_VERSION 3   /* 2: stats and options carry the persistent engine's
+#define GPUPR_ABI_VERSION 4   /* 2: stats and options carry the persistent engine's
                                  grid, relabel factor and chaining; tuning entries.
                                  3: stats carry the active-sweep time, the graphs
                                  a batch retired early and the bottom-up steps;
-                                 options carry the direction-optimizing BFS switch */
+                                 options carry the direction-optimizing BFS switch.
+                                 4: options carry relabel_tiles, stats the tile
+                                 steps (53 eight-byte stats fields) */
 
 typedef enum {
     GPUPR_OK = 0,
@@ -94,6 +96,11 @@ typedef struct {
     double bfs_ms_by_frontier[3];       /* ... and their time (block 0's clock) */
     uint64_t bfs_tail_steps;    /* BFS steps run by one block (bfs_tail_max) */
     uint64_t bfs_tail_levels;   /* ... and the levels they covered */
+    int64_t relabel_tiles;      /* persistent engine: 1 = the relabels ran by tiles */
+    uint64_t tile_steps;        /* tiled relabels: tile steps (grid barriers) */
+    uint64_t tile_procs;        /* ... tiles processed */
+    uint64_t tile_loads;        /* ... nodes those tiles loaded */
+    uint64_t tile_writes;       /* ... labels lowered */
 } gpupr_cut_stats;
 
 /* Solver tuning knobs; zero fields take the defaults shown. */
@@ -147,6 +154,14 @@ typedef struct {
                                      (bfs_chain_hops) only over frontiers of at
                                      most this many nodes (default: any frontier
                                      whose chained step fits the queue bound) */
+    int32_t relabel_tiles;        /* persistent engine: 1 = global relabels by
+                                     tiles of 2048 consecutive nodes, each
+                                     solved in shared memory and re-run when a
+                                     label it reads from another tile goes
+                                     down (exact distances, no in-arc rows);
+                                     < 0 = frontier steps; 0 = default (frontier
+                                     steps); bfs_bottom_up and bfs_tail_max
+                                     apply to frontier steps only */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

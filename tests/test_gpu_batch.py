@@ -28,14 +28,15 @@ def _run_batch(graphs, **kw):
     return toff, gpupr_capi.graph_cut_batch(toff, voff, V, t, n, L, 10.0, **kw)
 
 
-@pytest.mark.parametrize("engine,bottom_up,tail", [(1, 0, 0), (2, 0, 0), (2, 1, 0), (2, 0, 1024)])
-def test_batch_equals_individual_cuts(built, engine, bottom_up, tail):
+@pytest.mark.parametrize("engine,bottom_up,tail,tiles", [(1, 0, 0, 0), (2, 0, 0, 0), (2, 1, 0, 0),
+                                                         (2, 0, 1024, 0), (2, 0, 0, 1), (2, 0, 0, -1)])
+def test_batch_equals_individual_cuts(built, engine, bottom_up, tail, tiles):
     import gpupr_capi
 
     graphs = _graphs()
     toff, (out, items, st) = _run_batch(graphs, opts=gpupr_capi.options(
         engine=engine, bfs_bottom_up=bottom_up, bfs_bottom_up_ratio=1e9 if bottom_up else 0.0,
-        bfs_tail_max=tail))
+        bfs_tail_max=tail, relabel_tiles=tiles))
     assert len(items) == len(graphs)
     for k, g in enumerate(graphs):
         lab, ost = orc.graph_cut(g["vertices"], g["tets"], g["neighbors"], g["labels"], 10.0)

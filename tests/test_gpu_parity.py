@@ -107,7 +107,13 @@ def test_solver_invariants(built, kind, seed, size):
                                  dict(bfs_tail_max=1024, bfs_chain_hops=1, work_relabel_factor=0.05),
                                  dict(bfs_bottom_up=1), dict(bfs_bottom_up=1, bfs_bottom_up_ratio=64.0),
                                  dict(bfs_bottom_up=1, bfs_bottom_up_ratio=1e9, blocks_per_sm=1),
-                                 dict(bfs_bottom_up=1, bfs_bottom_up_ratio=1e9, work_relabel_factor=0.05)])
+                                 dict(bfs_bottom_up=1, bfs_bottom_up_ratio=1e9, work_relabel_factor=0.05),
+                                 dict(relabel_tiles=1), dict(relabel_tiles=-1),
+                                 dict(relabel_tiles=1, blocks_per_sm=1),
+                                 dict(relabel_tiles=1, work_relabel_factor=0.05),
+                                 dict(relabel_tiles=1, discharge_warp_aggregate=1),
+                                 dict(relabel_tiles=1, bfs_bottom_up=1, bfs_tail_max=1024),
+                                 dict(relabel_tiles=1, engine=1)])
 def test_options_do_not_change_the_cut(built, opt):
     import gpupr_capi
 

@@ -224,6 +224,11 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
     }
     st->bfs_tail_steps = sr.tail_steps;
     st->bfs_tail_levels = sr.tail_levels;
+    st->relabel_tiles = sr.relabel_tiles;
+    st->tile_steps = sr.tile_steps;
+    st->tile_procs = sr.tile_procs;
+    st->tile_loads = sr.tile_loads;
+    st->tile_writes = sr.tile_writes;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -551,6 +556,11 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
     }
     st->bfs_tail_steps = sr.tail_steps;
     st->bfs_tail_levels = sr.tail_levels;
+    st->relabel_tiles = sr.relabel_tiles;
+    st->tile_steps = sr.tile_steps;
+    st->tile_procs = sr.tile_procs;
+    st->tile_loads = sr.tile_loads;
+    st->tile_writes = sr.tile_writes;
     st->kernel_launches = launches;
     st->native_total_seconds = seconds_since(all0);
 }
@@ -800,6 +810,11 @@ gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_r
             }
             stats->bfs_tail_steps = sr.tail_steps;
             stats->bfs_tail_levels = sr.tail_levels;
+            stats->relabel_tiles = sr.relabel_tiles;
+            stats->tile_steps = sr.tile_steps;
+            stats->tile_procs = sr.tile_procs;
+            stats->tile_loads = sr.tile_loads;
+            stats->tile_writes = sr.tile_writes;
             stats->kernel_launches = launches;
         }
     });
@@ -871,6 +886,11 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
             }
             stats->bfs_tail_steps = sr.tail_steps;
             stats->bfs_tail_levels = sr.tail_levels;
+            stats->relabel_tiles = sr.relabel_tiles;
+            stats->tile_steps = sr.tile_steps;
+            stats->tile_procs = sr.tile_procs;
+            stats->tile_loads = sr.tile_loads;
+            stats->tile_writes = sr.tile_writes;
             stats->kernel_launches = launches;
         }
     });

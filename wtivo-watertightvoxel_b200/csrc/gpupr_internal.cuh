@@ -61,7 +61,18 @@ struct Ctl {
     unsigned long long step_ns[3];
     unsigned long long tail_steps;   // tail steps and the levels they covered
     unsigned long long tail_levels;
+    // tiled relabels: tile steps (grid barriers), tiles processed, nodes
+    // loaded by them and labels they lowered
+    unsigned long long tile_steps;
+    unsigned long long tile_procs;
+    unsigned long long tile_loads;
+    unsigned long long tile_writes;
 };
+
+// Nodes per tile of a tiled relabel (a power of two; the persistent engine
+// keeps one tile's labels and in-tile arcs in shared memory).
+constexpr uint32_t RELABEL_TILE_SHIFT = 11;
+constexpr uint32_t RELABEL_TILE = 1u << RELABEL_TILE_SHIFT;
 
 // Nodes per pass of a whole-array sweep (seed, excess init, active sweep):
 // 256 threads x 4 nodes.  Segmented solves keep the first graph of every such
@@ -115,6 +126,14 @@ struct SolveView {
     uint32_t tail_max;                  // persistent engine: frontiers up to this size are
                                         // expanded by block 0 alone, level after level
                                         // (0: never)
+    // Tiled relabels (persistent engine; arcm == null: frontier steps).  The
+    // nodes are cut into tiles of RELABEL_TILE consecutive ids; a relabel
+    // solves the BFS inside each tile in shared memory and re-queues a tile
+    // only when a label its nodes read from another tile went down.
+    uint8_t* arcm;                      // [n] per node: bit k = residual arc to neighbour k,
+                                        // bit 4+k = residual arc from it (seed sweep)
+    uint32_t* tile_stamp;               // [ntiles] last tile step the tile was queued for
+    uint32_t ntiles;
 };
 
 // ---------------------------------------------------------------------------
@@ -283,6 +302,8 @@ struct SolveOptions {
     double bfs_bottom_up_ratio = 1.0;
     int max_blocks_per_sm = 0;     // persistent engine: cap on the grid (0 = none); the
                                    // server's lanes use it so their solves fit side by side
+    int relabel_tiles = 0;         // persistent engine: 1 = tiled relabels, < 0 = frontier
+                                   // steps, 0 = default
 };
 
 SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw,
@@ -296,11 +317,13 @@ struct SolveWorkspace {
     DevBuf<uint32_t> chunk_seg, seg_live, seg_act;   // segmented solves only
     DevBuf<uint32_t> cand0, cand1;                   // direction-optimizing relabels only
     DevBuf<int4> inrow;                              // persistent engine: in-arc rows
+    DevBuf<uint8_t> arcm;                            // tiled relabels: arc masks
+    DevBuf<uint32_t> tile_stamp;                     // tiled relabels: queue stamps
     uint64_t bytes() const
     {
         return excess.bytes() + height.bytes() + q0.bytes() + q1.bytes() + q2.bytes() + ctl.bytes() +
                chunk_seg.bytes() + seg_live.bytes() + seg_act.bytes() + cand0.bytes() + cand1.bytes() +
-               inrow.bytes();
+               inrow.bytes() + arcm.bytes() + tile_stamp.bytes();
     }
 };
 
@@ -328,6 +351,8 @@ struct SolveResult {
     int blocks_per_sm = 0;         // persistent engine: grid used
     double work_factor = 0.0;      // persistent engine: relabel work factor used
     int chain_hops = 0, chain_max_active = 0;   // persistent engine: chaining used
+    int relabel_tiles = 0;         // persistent engine: 1 = tiled relabels ran
+    uint64_t tile_steps = 0, tile_procs = 0, tile_loads = 0, tile_writes = 0;
 };
 
 // Autotuner table (push_relabel.cu): per size class (floor(log2 n)), the

@@ -33,6 +33,9 @@
 //  * Queue appends are staged in shared memory and written with one global
 //    atomic per block iteration; sink flow and work counters are reduced per
 //    block.
+//  * As an option, relabels by tiles of consecutive nodes: each tile's BFS
+//    runs in shared memory and a tile is re-run only when a label it reads
+//    from another tile goes down (exact distances at the fixpoint).
 //  * Exactness by construction: the solve ends only when a global relabel
 //    (reachability exact) finds no node with excess that can reach the sink, so the
 //    returned preflow is maximum and the sink-reachable set is the minimal
@@ -155,6 +158,39 @@ __device__ __forceinline__ int4 in_arc_row(const SolveView& g, uint32_t u)
                      p4.w > r4.w ? nb4.w : -1);
 }
 
+// A node's arc mask for a tiled relabel: bit k = residual arc v -> nbr[v][k]
+// (res > 0), bit 4+k = residual arc nbr[v][k] -> v (pair - res > 0), both
+// exact between phases.
+__device__ __forceinline__ uint32_t arc_mask(const SolveView& g, uint32_t v)
+{
+    const int4 nb4 = __ldg(g.nbr + v);
+    const uint4 p4 = __ldg(g.pair + v);
+    const uint4 r4 = __ldcg(reinterpret_cast<const uint4*>(g.res) + v);
+    const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+    const uint32_t r[4] = {r4.x, r4.y, r4.z, r4.w}, pr[4] = {p4.x, p4.y, p4.z, p4.w};
+    uint32_t m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (nb[k] < 0) continue;
+        m |= (uint32_t)(r[k] > 0u) << k;
+        m |= (uint32_t)(pr[k] > r[k]) << (4 + k);
+    }
+    return m;
+}
+
+// Queues tile t for tile step `step` unless it is queued for it already (the
+// stamp holds the last step a tile was queued for; steps only grow within a
+// solve, so each tile enters a step's queue at most once and the queue,
+// RELABEL_TILE-fold shorter than a node queue, cannot overflow).
+__device__ __forceinline__ void queue_tile(const SolveView& g, uint32_t t, uint32_t step)
+{
+    if (atomicMax(g.tile_stamp + t, step) >= step) return;
+    uint32_t* q = (step & 1u) ? g.fr[1] : g.fr[0];
+    const uint32_t pos = atomicAdd(&g.ctl->bfs_cnt[step % 3u], 1u);
+    if (pos < g.ntiles) q[pos] = t;
+    else raise_error(g.ctl, (int)GPUPR_ERR_INVARIANT);
+}
+
 // Level 1 of the backward BFS: nodes with a residual arc to the sink.  Every
 // other height is reset to UNVIS (.cu:374-379).  With g.inrow (persistent
 // engine) the same streaming pass writes every node's in-arc row, so a BFS
@@ -163,9 +199,12 @@ __device__ __forceinline__ int4 in_arc_row(const SolveView& g, uint32_t u)
 // s_fr and s_act hold DTPB * SWEEP_UNROLL entries each.  With kActive the
 // seeds that hold excess are appended to the active queue (engine 1; the
 // persistent engine finds the active nodes after the BFS, active_sweep_body).
+// With g.arcm (tiled relabels) the pass writes every node's arc mask instead
+// of an in-arc row and queues the tiles holding a seed for tile step
+// `tile_step`; the seeds are not appended to a frontier.
 template <bool kActive>
 __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr, uint32_t* s_act,
-                                              uint32_t* s_m)
+                                              uint32_t* s_m, uint32_t tile_step = 0u)
 {
     Ctl* ctl = g.ctl;
     constexpr uint32_t CH = DTPB * SWEEP_UNROLL;
@@ -186,6 +225,18 @@ __device__ __forceinline__ void bfs_seed_body(const SolveView& g, uint32_t* s_fr
             const uint32_t v = base + j * DTPB + threadIdx.x;
             x[j] = (kActive && in[j] && t[j] < 0) ? ldcg(g.excess + v) : 0ll;
             if (in[j]) g.height[v] = (t[j] < 0) ? 1u : UNVIS;
+        }
+        if (g.arcm) {
+            // a warp's 32 nodes lie in one tile (RELABEL_TILE is a multiple of 32)
+#pragma unroll
+            for (int j = 0; j < SWEEP_UNROLL; ++j) {
+                const uint32_t v = base + j * DTPB + threadIdx.x;
+                if (in[j]) g.arcm[v] = (uint8_t)arc_mask(g, v);
+                const unsigned seeds = __ballot_sync(0xffffffffu, in[j] && t[j] < 0);
+                if (seeds && (int)(threadIdx.x & 31u) == __ffs(seeds) - 1)
+                    queue_tile(g, v >> RELABEL_TILE_SHIFT, tile_step);
+            }
+            continue;   // no frontier: the tile steps start from the queued tiles
         }
         if (g.inrow) {
 #pragma unroll 2
@@ -545,12 +596,276 @@ __device__ __forceinline__ void bfs_step_body(const SolveView& g, uint32_t L, ui
     }
 }
 
+// ---------------------------------------------------------------------------
+// Tiled relabels (persistent engine).  A frontier step costs a grid barrier
+// and a few dependent round trips per node however few nodes it labels, and a
+// relabel of the benchmark graph takes ~300 of them.  Here the nodes are cut
+// into tiles of RELABEL_TILE consecutive ids (node order is spatial, so most
+// arcs stay inside a tile); a tile step gives every queued tile to one block,
+// which loads the tile's labels and in-tile arcs into shared memory, lowers
+// the labels from the tile's arcs into other tiles, runs the BFS inside the
+// tile from the nodes that went down, in rounds of shared-memory worklists
+// with block syncs, writes the labels that went down and
+// queues, for the next step, every other tile with a node whose arc into a
+// lowered node now offers a label below its own.  Labels only go down and
+// each is the length of a real path to the sink; when a step's queue is empty
+// no residual arc u -> v has h(u) > h(v) + 1, so the labels are the exact
+// BFS distances and reachability is exact.  Each tile is written by one block
+// in a step (the stamps keep a tile once per queue); labels read from other
+// tiles may be older than the last write, which only re-queues a tile.
+// ---------------------------------------------------------------------------
+static_assert(RELABEL_TILE == DTPB * 8u, "a tile's labels fill the solver's staging buffer");
+
+// Shared memory of one tile, after the solver's static staging buffer (which
+// holds the tile's labels): per node the tile offsets of its in-arc sources
+// inside the tile (four 16-bit offsets, 0xFFFF = none), its arc mask, a flag
+// "label went down", and a list of 16-bit entries: the (node, slot) pairs
+// whose arc leaves the tile (node << 2 | slot), or, while the BFS inside the
+// tile runs, two worklists of nodes.  A tile's neighbour rows are read once,
+// coalesced, per processing.
+constexpr uint32_t TILE_LIST_CAP = 2u * RELABEL_TILE;
+constexpr size_t TILE_SMEM = (size_t)RELABEL_TILE * 8u       // in-tile in-arc sources
+                             + (size_t)RELABEL_TILE           // arc masks
+                             + (size_t)RELABEL_TILE           // lowered flags
+                             + (size_t)TILE_LIST_CAP * 2u;    // list / worklists
+struct TileSmem {
+    uint2* tin;
+    uint8_t* am;
+    uint8_t* low;
+    uint16_t* list;
+};
+// Nodes one thread may take in a row in a round of the BFS inside a tile.
+constexpr int TILE_CHAIN = 4;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Index for this lane's entry in a shared list whose size is *s_cnt, one
+// shared atomic per warp; every active lane calls it, `want` or not.
+__device__ __forceinline__ uint32_t warp_list_index(bool want, uint32_t* s_cnt)
+{
+    const unsigned act = __activemask();
+    const unsigned bal = __ballot_sync(act, want);
+    if (!bal) return 0xFFFFFFFFu;
+    const int leader = __ffs(bal) - 1;
+    const int lane = (int)(threadIdx.x & 31u);
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(s_cnt, (uint32_t)__popc(bal));
+    base = __shfl_sync(act, base, leader);
+    return want ? base + (uint32_t)__popc(bal & ((1u << lane) - 1u)) : 0xFFFFFFFFu;
+}
+
+// One tile of tile step `step`, by the whole block.  s_lab: RELABEL_TILE
+// labels; s_tc: four shared words (list and worklist sizes, overflow
+// flags).  In the first step of a relabel (`first`) every labelled node of
+// the tile announces its label to the other tiles: a seed is labelled by the
+// seed sweep, before the step, so its label never goes down here.
+__device__ __forceinline__ void tile_relabel(const SolveView& g, uint32_t t, uint32_t step, bool first,
+                                             uint32_t* s_lab, const TileSmem& sm, uint32_t* s_tc,
+                                             unsigned long long& writes, unsigned long long& levels)
+{
+    const uint32_t b = t << RELABEL_TILE_SHIFT;
+    const uint32_t m = min(RELABEL_TILE, g.n - b);
+    const int4* rows = g.nbr + b;
+    // ---- the tile's labels and masks, 16 bytes a copy, all in flight ----
+    const uint32_t m4 = m >> 2, m16 = m >> 4;   // whole 16-byte chunks inside the arrays
+    for (uint32_t c = threadIdx.x; c < m4; c += DTPB) cp_async16(s_lab + 4u * c, g.height + b + 4u * c);
+    for (uint32_t c = threadIdx.x; c < m16; c += DTPB) cp_async16(sm.am + 16u * c, g.arcm + b + 16u * c);
+    for (uint32_t j = 4u * m4 + threadIdx.x; j < m; j += DTPB) s_lab[j] = ldcg(g.height + b + j);
+    for (uint32_t j = 16u * m16 + threadIdx.x; j < m; j += DTPB) sm.am[j] = __ldcg(g.arcm + b + j);
+    for (uint32_t j = threadIdx.x; j < m; j += DTPB) sm.low[j] = 0u;
+    if (threadIdx.x < 4) s_tc[threadIdx.x] = 0u;
+    cp_async_wait_all();
+    __syncthreads();
+    // ---- one pass over the rows (four rows of a thread in flight at once):
+    // in-tile in-arc sources, and the arcs into other tiles listed ----
+    for (uint32_t j0 = threadIdx.x; j0 < m; j0 += 4u * DTPB) {
+        int4 rr[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t j = j0 + (uint32_t)k * DTPB;
+            rr[k] = (j < m && sm.am[j]) ? __ldg(rows + j) : make_int4(-1, -1, -1, -1);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t j = j0 + (uint32_t)k * DTPB;
+            if (j >= m) break;   // j grows with k: the lanes past m stay past it
+            const uint32_t am = sm.am[j];
+            const int nb[4] = {rr[k].x, rr[k].y, rr[k].z, rr[k].w};
+            uint32_t loc[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t off = (uint32_t)nb[q] - b;
+                loc[q] = (((am >> (4 + q)) & 1u) && off < m) ? off : 0xFFFFu;
+                const bool x = ((am >> q) & 1u) && off >= m;
+                const uint32_t i = warp_list_index(x, &s_tc[0]);
+                if (x && i < TILE_LIST_CAP) sm.list[i] = (uint16_t)((j << 2) | (uint32_t)q);
+                else if (x) {   // list full: this one at once
+                    const uint32_t hv = ldcg(g.height + nb[q]);
+                    if (hv != UNVIS && atomicMin(s_lab + j, hv + 1u) > hv + 1u) sm.low[j] = 1u;
+                }
+            }
+            sm.tin[j] = make_uint2(loc[0] | (loc[1] << 16), loc[2] | (loc[3] << 16));
+        }
+    }
+    __syncthreads();
+    // ---- lower each listed source node from the other tile's label, all
+    // loads of a thread in flight at once ----
+    const uint32_t npull = min(s_tc[0], TILE_LIST_CAP);
+    for (uint32_t i0 = 0; i0 < npull; i0 += 4u * DTPB) {
+        uint32_t e[4], hv[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t i = i0 + (uint32_t)k * DTPB + threadIdx.x;
+            e[k] = i < npull ? sm.list[i] : 0xFFFFFFFFu;
+            hv[k] = UNVIS;
+            if (e[k] != 0xFFFFFFFFu) {
+                const int4 r = __ldg(rows + (e[k] >> 2));
+                const int nb[4] = {r.x, r.y, r.z, r.w};
+                hv[k] = ldcg(g.height + nb[e[k] & 3u]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (hv[k] == UNVIS) continue;
+            const uint32_t j = e[k] >> 2;
+            if (atomicMin(s_lab + j, hv[k] + 1u) > hv[k] + 1u) sm.low[j] = 1u;
+        }
+    }
+    // ---- the BFS inside the tile, by worklists: a node whose label went down
+    // (or, in the first step, every labelled node) offers label + 1 to its
+    // in-tile in-arc sources; a source that takes it is expanded next by the
+    // same thread (up to TILE_CHAIN in a row) or listed for the next round.
+    // Only the tile's own block writes its labels, so the tile was at a
+    // fixpoint after its last processing and only these nodes can move it.
+    // A list that overflows makes the next round expand every node. ----
+    __syncthreads();   // the pull list is consumed: its space holds the worklists
+    if (threadIdx.x == 0) s_tc[0] = 0u;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < m; j += DTPB) {
+        const bool x = sm.low[j] || (first && s_lab[j] != UNVIS);
+        const uint32_t i = warp_list_index(x, &s_tc[0]);
+        if (x) sm.list[i] = (uint16_t)j;   // at most m entries
+    }
+    __syncthreads();
+    for (uint32_t r = 0;; ++r) {
+        const uint32_t c = min(s_tc[r & 1u], RELABEL_TILE);
+        const bool full = s_tc[2u + (r & 1u)] != 0u;
+        __syncthreads();   // every thread has read this round's counts
+        if (c == 0u && !full) break;
+        if (r > g.n + 2u) {   // every round lowers a label: a broken invariant
+            if (threadIdx.x == 0) raise_error(g.ctl, (int)GPUPR_ERR_INVARIANT);
+            break;
+        }
+        const uint32_t nx = (r + 1u) & 1u;
+        if (threadIdx.x == 0) {
+            s_tc[nx] = 0u;
+            s_tc[2u + nx] = 0u;
+        }
+        __syncthreads();
+        const uint32_t cnt = full ? m : c;
+        for (uint32_t i = threadIdx.x; i < cnt; i += DTPB) {
+            uint32_t v = full ? i : sm.list[(r & 1u) * RELABEL_TILE + i];
+            for (int hop = 1;; ++hop) {
+                const uint32_t nl = s_lab[v] + 1u;
+                if (nl == 0u) break;   // unlabelled (UNVIS + 1 wraps)
+                const uint2 p = sm.tin[v];
+                const uint32_t src[4] = {p.x & 0xFFFFu, p.x >> 16, p.y & 0xFFFFu, p.y >> 16};
+                uint32_t old[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)   // four independent atomics in flight
+                    old[q] = src[q] != 0xFFFFu ? atomicMin(s_lab + src[q], nl) : 0u;
+                uint32_t next = 0xFFFFFFFFu;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t u = src[q];
+                    if (old[q] <= nl) continue;
+                    sm.low[u] = 1u;
+                    if (next == 0xFFFFFFFFu && hop < TILE_CHAIN) {
+                        next = u;
+                        continue;
+                    }
+                    const uint32_t k = atomicAdd(&s_tc[nx], 1u);
+                    if (k < RELABEL_TILE) sm.list[nx * RELABEL_TILE + k] = (uint16_t)u;
+                    else s_tc[2u + nx] = 1u;
+                }
+                if (next == 0xFFFFFFFFu) break;
+                v = next;
+            }
+        }
+        ++levels;
+        __syncthreads();
+    }
+    // ---- write the labels that went down; list their arcs from other tiles ----
+    if (threadIdx.x == 0) s_tc[0] = 0u;
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < m; j += DTPB) {
+        const uint32_t h = s_lab[j];
+        const bool lowered = sm.low[j] != 0u;
+        if (lowered) {
+            g.height[b + j] = h;
+            ++writes;
+        }
+        // in-arcs from other tiles: an in-arc bit whose source is not in the tile
+        const uint2 p = sm.tin[j];
+        const uint32_t src[4] = {p.x & 0xFFFFu, p.x >> 16, p.y & 0xFFFFu, p.y >> 16};
+        const uint32_t in = (lowered || (first && h != UNVIS)) ? (uint32_t)(sm.am[j] >> 4) : 0u;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const bool x = ((in >> q) & 1u) && src[q] == 0xFFFFu;
+            const uint32_t i = warp_list_index(x, &s_tc[0]);
+            if (x && i < TILE_LIST_CAP) sm.list[i] = (uint16_t)((j << 2) | (uint32_t)q);
+            else if (x) {   // list full: this one at once
+                const int4 r = __ldg(rows + j);
+                const int nb[4] = {r.x, r.y, r.z, r.w};
+                if (ldcg(g.height + nb[q]) > h + 1u)
+                    queue_tile(g, (uint32_t)nb[q] >> RELABEL_TILE_SHIFT, step + 1u);
+            }
+        }
+    }
+    __syncthreads();
+    // ---- queue the other tiles whose node now has a shorter way out ----
+    const uint32_t nnote = min(s_tc[0], TILE_LIST_CAP);
+    for (uint32_t i0 = 0; i0 < nnote; i0 += 4u * DTPB) {
+        uint32_t w[4], hw[4], e[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t i = i0 + (uint32_t)k * DTPB + threadIdx.x;
+            e[k] = i < nnote ? sm.list[i] : 0xFFFFFFFFu;
+            w[k] = 0xFFFFFFFFu;
+            hw[k] = 0u;
+            if (e[k] != 0xFFFFFFFFu) {
+                const int4 r = __ldg(rows + (e[k] >> 2));
+                const int nb[4] = {r.x, r.y, r.z, r.w};
+                w[k] = (uint32_t)nb[e[k] & 3u];
+                hw[k] = ldcg(g.height + w[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (w[k] == 0xFFFFFFFFu || hw[k] <= s_lab[e[k] >> 2] + 1u) continue;
+            const uint32_t tw = w[k] >> RELABEL_TILE_SHIFT;
+            if (ldcg(g.tile_stamp + tw) < step + 1u) queue_tile(g, tw, step + 1u);
+        }
+    }
+    __syncthreads();   // the shared tile is the next tile's
+}
+
 // Frontier entries block 0 keeps in shared memory in a tail step, and the
 // most levels one tail step covers (a bound on the other blocks' barrier wait).
 constexpr uint32_t TAIL_CAP = DTPB * 4u;
 constexpr int TAIL_LEVELS = 4096;
 // Default frontier size up to which tail steps run (0: none).
 constexpr uint32_t BFS_TAIL_DEFAULT = 0u;
+// Free nodes from which the persistent engine relabels by tiles by default.
+constexpr uint32_t RELABEL_TILES_DEFAULT_MIN = 0xFFFFFFFFu;
 
 // A tail step of the persistent engine's BFS, run by block 0 alone while the
 // other blocks wait at the grid barrier: starting from level L0's frontier
@@ -965,10 +1280,12 @@ __device__ bool grid_barrier(Ctl* ctl, unsigned long long& target, unsigned long
 }
 
 // kAgg: warp-aggregated excess atomics in the discharge (an option).
-template <bool kAgg>
+// kTiles: tiled relabels (g.arcm set), a separate instantiation so that the
+// frontier-step kernel keeps its registers.
+template <bool kAgg, bool kTiles>
 __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, PersistParams p)
 {
-    __shared__ uint32_t s_buf[DTPB * 8];
+    __shared__ __align__(16) uint32_t s_buf[DTPB * 8];   // 16-byte copies land here (tiles)
     __shared__ uint32_t s_m[12];
     __shared__ unsigned long long s_red[DTPB / 32];
     __shared__ int s_ok;
@@ -978,6 +1295,21 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
     unsigned long long bar_target = 0;
     Work w;
     unsigned long long bfs_visits = 0;
+    // tiled relabels: the last tile step (the same in every block), tiles and
+    // nodes this block processed, labels this thread lowered
+    uint32_t tstep = 0;
+    unsigned long long tprocs = 0, tloads = 0, twrites = 0, tsteps = 0, tlevels = 0;
+    // tiled relabels: the tile's rows, masks, flags and list (TILE_SMEM bytes
+    // of dynamic shared memory; none in the other instantiations)
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    __shared__ uint32_t s_tc[kTiles ? 4 : 1];
+    TileSmem tsm{};
+    if (kTiles) {
+        tsm.tin = reinterpret_cast<uint2*>(s_dyn);
+        tsm.am = s_dyn + (size_t)RELABEL_TILE * 8u;
+        tsm.low = tsm.am + RELABEL_TILE;
+        tsm.list = reinterpret_cast<uint16_t*>(tsm.low + RELABEL_TILE);
+    }
     if (threadIdx.x < 12) s_m[threadIdx.x] = 0u;
     // phase clock of block 0, read after each phase's closing barrier:
     // s_clk = {BFS, active sweep, discharge, last mark} (shared memory, so it
@@ -1017,12 +1349,35 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
         }
         while (ok) {
             // ---- global relabel (label-correcting steps, reachability exact) ----
-            bfs_seed_body<false>(g, s_buf, s_buf + DTPB * 4, s_m);
+            bfs_seed_body<false>(g, s_buf, s_buf + DTPB * 4, s_m, kTiles ? tstep + 1u : 0u);
             if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
+            const uint32_t S0 = tstep + 1u;   // the seeds' tile step
+            while (kTiles) {
+                // ---- tile steps (tiled relabels) ----
+                const uint32_t S = ++tstep;
+                const uint32_t cnt = min(vload(&ctl->bfs_cnt[S % 3u]), g.ntiles);
+                if (cnt == 0) break;
+                if (lead) ctl->bfs_cnt[(S + 2u) % 3u] = 0u;
+                const uint32_t* tq = (S & 1u) ? g.fr[1] : g.fr[0];
+                for (uint32_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+                    const uint32_t t = __ldcg(tq + i);
+                    if (t >= g.ntiles) {   // queue entries are tile ids by construction
+                        if (threadIdx.x == 0) raise_error(ctl, (int)GPUPR_ERR_INVARIANT);
+                        continue;
+                    }
+                    tile_relabel(g, t, S, S == S0, s_buf, tsm, s_tc, twrites, tlevels);
+                    ++tprocs;
+                    tloads += min(RELABEL_TILE, g.n - (t << RELABEL_TILE_SHIFT));
+                }
+                if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
+                ++levels_total;
+                ++tsteps;
+            }
+            if (!ok) break;
             uint32_t L = 1;
             bool exact = true;   // no chained step yet: every frontier node is labelled L
             uint32_t labelled = 0, bu_j = 0;
-            for (;;) {
+            for (; !kTiles;) {
                 const uint32_t first = prefetch_entry((L & 1) ? g.fr[1] : g.fr[0], g.n);
                 const uint32_t cnt = min(vload(&ctl->bfs_cnt[L % 3]), g.n);
                 if (cnt == 0) break;
@@ -1150,9 +1505,19 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
             ctl->bfs_ns = s_clk[0];
             ctl->sweep_ns = s_clk[1];
             ctl->discharge_ns = s_clk[2];
+            ctl->tile_steps = tsteps;
         }
     }
     reduce_work(ctl, w, bfs_visits, s_red);
+    if (kTiles) {
+        const unsigned long long x = warp_block_sum(twrites, s_red);
+        if (threadIdx.x == 0) {
+            if (x) atomicAdd(&ctl->tile_writes, x);
+            if (tlevels) atomicAdd(&ctl->bfs_visits, tlevels);   // levels run inside tiles
+            if (tprocs) atomicAdd(&ctl->tile_procs, tprocs);
+            if (tloads) atomicAdd(&ctl->tile_loads, tloads);
+        }
+    }
 }
 
 // First graph of every sweep chunk: the largest k with off[k] <= the chunk's
@@ -1267,6 +1632,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
         r.discharge_warp_aggregate = o->discharge_warp_aggregate;
         if (o->bfs_chain_max_frontier > 0) r.bfs_chain_max_frontier = o->bfs_chain_max_frontier;
         r.bfs_bottom_up = o->bfs_bottom_up;
+        r.relabel_tiles = o->relabel_tiles;
         if (o->bfs_bottom_up_ratio > 0) r.bfs_bottom_up_ratio = o->bfs_bottom_up_ratio;
     }
     // clamps of gpu_push_relabel_fast.cu:421-424 and :476-480
@@ -1284,7 +1650,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
 int persistent_blocks_per_sm()
 {
     int bps = 0;
-    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent<false>, DTPB, 0));
+    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent<false, false>, DTPB, 0));
     return bps;
 }
 
@@ -1305,7 +1671,14 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
 {
     using Clock = std::chrono::steady_clock;
     int bps = 0;
-    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_solve_persistent<false>, DTPB, 0));
+    const bool agg = opt.discharge_warp_aggregate > 0;
+    const void* kern = g.arcm ? (agg ? (const void*)k_solve_persistent<true, true>
+                                     : (const void*)k_solve_persistent<false, true>)
+                              : (agg ? (const void*)k_solve_persistent<true, false>
+                                     : (const void*)k_solve_persistent<false, false>);
+    const size_t dsmem = g.arcm ? TILE_SMEM : 0u;
+    if (dsmem) GPUPR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
+    GPUPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, DTPB, dsmem));
     if (bps < 1) throw Error{GPUPR_ERR_CUDA, "persistent solver kernel cannot be resident"};
     // resident blocks per SM: a step of a small graph is one chain of
     // dependent L2 round trips plus a grid barrier whose cost grows with the
@@ -1358,7 +1731,7 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     // autotuner may pick another setting.
     gv.chain_hops = opt.chain_hops > 0 ? opt.chain_hops : tuned ? te.chain_hops : 4;
     gv.bfs_hops = opt.bfs_chain_hops > 0 ? std::min(opt.bfs_chain_hops, 64) : BFS_CHAIN_HOPS;
-    gv.warp_agg = opt.discharge_warp_aggregate > 0 ? 1 : 0;
+    gv.warp_agg = agg ? 1 : 0;
     // BFS steps chain over frontiers of any size the queue bound allows
     // (measured against a 65,536-node limit: benchmark graph 78.3 -> 77.2 ms,
     // 3M-tet torus 2.30 -> 2.28 ms, 8M-tet open box 14.5 -> 14.0 ms)
@@ -1373,9 +1746,7 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
                           : g.n < 2000000u         ? 32768u
                                                    : 4096u;
     void* args[] = {&gv, &p};
-    const void* kern = gv.warp_agg ? (const void*)k_solve_persistent<true>
-                                   : (const void*)k_solve_persistent<false>;
-    GPUPR_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(DTPB), args, 0, s));
+    GPUPR_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(DTPB), args, dsmem, s));
     GPUPR_CUDA(cudaEventRecord(e1, s));
     GPUPR_CUDA(cudaMemcpyAsync(pc, g.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
     GPUPR_CUDA(cudaStreamSynchronize(s));
@@ -1412,6 +1783,11 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     out.bottom_up_steps = hc.bu_steps;
     out.tail_steps = hc.tail_steps;
     out.tail_levels = hc.tail_levels;
+    out.relabel_tiles = g.arcm ? 1 : 0;
+    out.tile_steps = hc.tile_steps;
+    out.tile_procs = hc.tile_procs;
+    out.tile_loads = hc.tile_loads;
+    out.tile_writes = hc.tile_writes;
     for (int k = 0; k < 3; ++k) {
         out.step_cnt[k] = hc.step_cnt[k];
         out.step_ms[k] = (double)hc.step_ns[k] * 1e-6;
@@ -1476,10 +1852,22 @@ void solve_push_relabel(uint32_t n, const int4* d_nbr, uint32_t* d_res, const ui
             g.seg_act = w.seg_act.p;
             out.workspace_bytes = w.bytes();
         }
-        if (w.inrow.n < n) w.inrow = DevBuf<int4>(n, s);
-        g.inrow = w.inrow.p;
+        const bool tiles = opt.relabel_tiles > 0 ||
+                           (opt.relabel_tiles == 0 && n >= RELABEL_TILES_DEFAULT_MIN);
+        if (tiles) {
+            const uint32_t nt = (uint32_t)(((uint64_t)n + RELABEL_TILE - 1u) >> RELABEL_TILE_SHIFT);
+            if (w.arcm.n < n) w.arcm = DevBuf<uint8_t>(n, s);
+            if (w.tile_stamp.n < nt) w.tile_stamp = DevBuf<uint32_t>(nt, s);
+            GPUPR_CUDA(cudaMemsetAsync(w.tile_stamp.p, 0, (size_t)nt * 4u, s));
+            g.arcm = w.arcm.p;
+            g.tile_stamp = w.tile_stamp.p;
+            g.ntiles = nt;
+        } else {
+            if (w.inrow.n < n) w.inrow = DevBuf<int4>(n, s);
+            g.inrow = w.inrow.p;
+        }
         out.workspace_bytes = w.bytes();
-        if (opt.bfs_bottom_up) {
+        if (opt.bfs_bottom_up && !tiles) {
             if (w.cand0.n < n) {
                 w.cand0 = DevBuf<uint32_t>(n, s);
                 w.cand1 = DevBuf<uint32_t>(n, s);

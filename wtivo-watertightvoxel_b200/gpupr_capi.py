@@ -41,6 +41,9 @@ STATS_FIELDS = [
     ("bottom_up_steps", ctypes.c_uint64),
     ("bfs_steps_by_frontier", ctypes.c_uint64 * 3), ("bfs_ms_by_frontier", ctypes.c_double * 3),
     ("bfs_tail_steps", ctypes.c_uint64), ("bfs_tail_levels", ctypes.c_uint64),
+    ("relabel_tiles", ctypes.c_int64), ("tile_steps", ctypes.c_uint64),
+    ("tile_procs", ctypes.c_uint64), ("tile_loads", ctypes.c_uint64),
+    ("tile_writes", ctypes.c_uint64),
 ]
 
 
@@ -63,6 +66,7 @@ class SolveOptions(ctypes.Structure):
         ("bfs_bottom_up", ctypes.c_int32), ("bfs_bottom_up_ratio", ctypes.c_double),
         ("bfs_chain_hops", ctypes.c_int32), ("bfs_tail_max", ctypes.c_int32),
         ("discharge_warp_aggregate", ctypes.c_int32), ("bfs_chain_max_frontier", ctypes.c_int32),
+        ("relabel_tiles", ctypes.c_int32),
     ]
 
 
