@@ -131,7 +131,11 @@ int orc_surface(const uint8_t* labels, const double* V, uint64_t nv,
  * face contributes its three undirected edges as keys (min << 32 | max),
  * the keys are sorted, and each run of equal keys whose length is not 2 is
  * one bad edge group.  A closed 2-manifold mesh has none.  Returns ORC_OK or
- * ORC_ERR_NEG_VERTEX. */
+ * ORC_ERR_NEG_VERTEX.  The reference function needs CGAL/TBB to build; its
+ * own known-answer case (scripts/verify_install.py:38-41, a tetrahedron
+ * shell: watertight, 0 bad groups) pins this restatement in the tests.
+ * Parity of the label sampler below is unpinned: it follows OpenVDB's
+ * published BoxSampler, and no OpenVDB is present to compare against. */
 int orc_edge_audit(const int32_t* faces, uint64_t nf, uint64_t* bad_groups);
 
 /* Sparse unsigned distance grid of 8^3-voxel bricks (host arrays): voxel

@@ -212,7 +212,11 @@ def audit_cases():
     V, F = synth.icosphere(3)
     tet = np.array([[0, 1, 2], [0, 3, 1], [1, 3, 2], [2, 3, 0]], np.int32)
     soup = rng.integers(0, 50, size=(400, 3)).astype(np.int32)
+    # the reference's own known-answer case (scripts/verify_install.py:38-41):
+    # a tetrahedron shell, every edge of degree 2, so watertight with 0 bad groups
+    ref_shell = np.array([[0, 2, 1], [0, 1, 3], [0, 3, 2], [1, 2, 3]], np.int32)
     return {
+        "reference_install_check_tetra_shell": (ref_shell, 0),
         "closed_icosphere": (F, 0),
         "closed_tetrahedron": (tet, 0),
         "one_face_missing": (F[1:], 3),
