@@ -117,8 +117,9 @@ typedef struct {
     int32_t bfs_batch;            /* BFS levels enqueued per host check, default 48 */
     int32_t block_size;           /* threads per block, default 256 */
     int32_t blocks_per_sm;        /* resident blocks per SM; default: 4 (one
-                                     launch per step), by graph size 1..4
-                                     (persistent) */
+                                     launch per step), by graph size 2..4
+                                     (persistent: 2 below 1.5M free nodes, 3
+                                     below 5M, else 4) */
     double work_relabel_factor;   /* relabel after this many node visits per
                                      free node since the last one; default 3
                                      (one launch per step); persistent: 2 below
@@ -162,6 +163,13 @@ typedef struct {
                                      < 0 = frontier steps; 0 = default (frontier
                                      steps); bfs_bottom_up and bfs_tail_max
                                      apply to frontier steps only */
+    int32_t bfs_block_levels;     /* persistent engine: each BFS step expands its
+                                     frontier and then, per block and without a
+                                     grid barrier, up to this many levels in all
+                                     from the nodes the block labelled itself
+                                     (breadth first, shared-memory stage);
+                                     0 = default (16), 1 = per-thread chains
+                                     instead (bfs_chain_hops, bfs_chain_max_frontier) */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

@@ -1,4 +1,5 @@
-"""A host model of the persistent engine's BFS steps (bfs_step_body in
+"""A host model of the persistent engine's BFS steps (bfs_step_body, the
+per-thread chains, and bfs_step_levels_body, the block sub-levels, in
 csrc/push_relabel.cu), checked against a plain level-synchronous BFS.
 
 The device code runs a step's queue entries in parallel; the model runs them
@@ -147,4 +148,99 @@ def test_without_propagation_reachability_stays_exact(seed):
     assert not all_prop
     assert np.array_equal(h != UNVIS, ref != UNVIS)
     assert np.all(h[ref != UNVIS] >= ref[ref != UNVIS])   # path lengths, never below
+    assert once.max() <= 1
+
+
+def model_bfs_levels(nbr, res, seeds, rng, levels, blocks, half, threads=4):
+    """The step loop of k_solve_persistent's relabel with bfs_step_levels_body:
+    a step deals its frontier to `blocks` blocks of `threads` threads (one
+    entry per thread per pass); each block expands its entries, then, for up
+    to levels - 1 sub-levels, the nodes it staged itself (stage halves of
+    `half` entries; a node that does not fit goes to the next step's queue);
+    the last sub-level's stage goes to the next step's queue.  Blocks run one
+    after another in a random order, nodes within a sub-level too."""
+    n = len(nbr)
+    h = np.full(n, UNVIS, np.uint64)
+    frontier = [int(s) for s in np.nonzero(seeds)[0]]
+    h[frontier] = 1
+    queued_once = np.zeros(n, np.int64)
+    queued_once[frontier] += 1
+    steps, all_prop = 0, True
+    while frontier:
+        cnt = len(frontier)
+        passes = -(-cnt // (blocks * threads))
+        ex_max = cnt + (levels - 1) * half * blocks * passes
+        propagate = 4 * ex_max <= n
+        all_prop = all_prop and propagate
+        out, expanded = [], 0
+
+        def expand(u, stage):
+            nonlocal expanded
+            expanded += 1
+            cand = int(h[u]) + 1
+            for k in range(4):
+                v = nbr[u, k]
+                if v < 0 or not reverse_residual(nbr, res, u, k) or h[v] <= cand:
+                    continue
+                old = int(h[v])
+                h[v] = cand                           # atomicMin, won
+                if old != UNVIS and not propagate:
+                    continue
+                if old == UNVIS:
+                    queued_once[v] += 1
+                if len(stage) < half:
+                    stage.append(int(v))
+                else:
+                    out.append(int(v))                # the stage half is full
+
+        for p in range(passes):
+            for b in rng.permutation(blocks):
+                lo = (p * blocks + b) * threads
+                cur = []
+                for i in rng.permutation(range(lo, min(lo + threads, cnt))) if lo < cnt else []:
+                    expand(frontier[i], cur)
+                for _ in range(levels - 1):
+                    if not cur:
+                        break
+                    nxt = []
+                    for u in rng.permutation(cur):
+                        expand(int(u), nxt)
+                    cur = nxt
+                out.extend(cur)
+        assert expanded <= ex_max
+        assert len(out) <= 4 * ex_max
+        if propagate:
+            assert len(out) <= n                      # the queue holds n entries
+        frontier = out
+        steps += 1
+    return h, steps, queued_once, all_prop
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("levels,half", [(2, 8), (4, 16), (16, 8), (16, 4)])
+def test_block_sublevels_reach_exactly_and_converge(seed, levels, half):
+    # sizes where every step's worst case fits the queue, so lowered labels propagate
+    rng = np.random.default_rng(200 + seed)
+    nbr, res, seeds = grid_graph(rng, 80, 60)
+    ref = bfs_distances(nbr, res, seeds)
+    h, steps, once, all_prop = model_bfs_levels(nbr, res, seeds, rng, levels, blocks=3, half=half,
+                                                threads=64)
+    assert np.array_equal(h != UNVIS, ref != UNVIS)   # reachability exact in every case
+    assert np.all(h[ref != UNVIS] >= ref[ref != UNVIS])
+    if all_prop or levels <= 4:                       # (the small cases always propagate here)
+        assert all_prop
+        assert np.array_equal(h, ref)                 # lowered labels propagated: distances
+    assert once.max() <= 1
+    assert steps < int(ref[ref != UNVIS].max())       # sub-levels cover several levels a step
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_block_sublevels_without_propagation_stay_exact(seed):
+    rng = np.random.default_rng(300 + seed)
+    nbr, res, seeds = grid_graph(rng, 24, 20, p_sink=0.3)
+    ref = bfs_distances(nbr, res, seeds)
+    h, _, once, all_prop = model_bfs_levels(nbr, res, seeds, rng, 16, blocks=8, half=64)
+    assert not all_prop
+    assert np.array_equal(h != UNVIS, ref != UNVIS)
+    assert np.all(h[ref != UNVIS] >= ref[ref != UNVIS])
     assert once.max() <= 1

@@ -98,13 +98,13 @@ def test_solver_invariants(built, kind, seed, size):
                                  dict(engine=2, global_relabel_period=-1, work_relabel_factor=0.1),
                                  dict(chain_hops=1), dict(chain_hops=2), dict(chain_hops=64),
                                  dict(chain_hops=64, local_steps=1, blocks_per_sm=1),
-                                 dict(bfs_chain_hops=1), dict(bfs_chain_hops=16),
+                                 dict(bfs_block_levels=1, bfs_chain_hops=1), dict(bfs_block_levels=1, bfs_chain_hops=16),
                                  dict(bfs_tail_max=1024), dict(bfs_tail_max=8, blocks_per_sm=1),
                                  dict(discharge_warp_aggregate=1),
-                                 dict(bfs_chain_max_frontier=1 << 30),
-                                 dict(bfs_chain_max_frontier=1 << 30, bfs_chain_hops=8),
+                                 dict(bfs_block_levels=1, bfs_chain_max_frontier=1 << 30),
+                                 dict(bfs_block_levels=1, bfs_chain_max_frontier=1 << 30, bfs_chain_hops=8),
                                  dict(discharge_warp_aggregate=1, chain_hops=1, local_steps=32),
-                                 dict(bfs_tail_max=1024, bfs_chain_hops=1, work_relabel_factor=0.05),
+                                 dict(bfs_tail_max=1024, bfs_block_levels=1, bfs_chain_hops=1, work_relabel_factor=0.05),
                                  dict(bfs_bottom_up=1), dict(bfs_bottom_up=1, bfs_bottom_up_ratio=64.0),
                                  dict(bfs_bottom_up=1, bfs_bottom_up_ratio=1e9, blocks_per_sm=1),
                                  dict(bfs_bottom_up=1, bfs_bottom_up_ratio=1e9, work_relabel_factor=0.05),
@@ -113,7 +113,9 @@ def test_solver_invariants(built, kind, seed, size):
                                  dict(relabel_tiles=1, work_relabel_factor=0.05),
                                  dict(relabel_tiles=1, discharge_warp_aggregate=1),
                                  dict(relabel_tiles=1, bfs_bottom_up=1, bfs_tail_max=1024),
-                                 dict(relabel_tiles=1, engine=1)])
+                                 dict(relabel_tiles=1, engine=1),
+                                 dict(bfs_block_levels=1), dict(bfs_block_levels=4), dict(bfs_block_levels=2, blocks_per_sm=1),
+                                 dict(bfs_block_levels=16, work_relabel_factor=0.05)])
 def test_options_do_not_change_the_cut(built, opt):
     import gpupr_capi
 

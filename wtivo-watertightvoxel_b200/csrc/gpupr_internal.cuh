@@ -106,6 +106,8 @@ struct SolveView {
     int chain_hops;                     // nodes one thread may discharge in a row in
                                         // one round (<= 1: no chaining) ...
     uint32_t chain_max_active;          // ... in rounds of at most this many nodes
+    int bfs_block_levels;               // persistent engine: > 1 = BFS steps expand that many
+                                        // levels per block from its shared stage (0: chains)
     int bfs_hops;                       // nodes one thread may label in a row in one
                                         // short BFS step (<= 1: level by level)
     // Segmented solve (a batch: independent graphs, each a contiguous node
@@ -304,6 +306,7 @@ struct SolveOptions {
                                    // server's lanes use it so their solves fit side by side
     int relabel_tiles = 0;         // persistent engine: 1 = tiled relabels, < 0 = frontier
                                    // steps, 0 = default
+    int bfs_block_levels = 0;      // persistent engine: > 1 = block sub-levels per BFS step
 };
 
 SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw,

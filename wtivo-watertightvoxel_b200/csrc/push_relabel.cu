@@ -13,8 +13,10 @@
 //  * Chained discharge: the thread that takes ownership of a neighbour's
 //    excess may discharge it at once, so excess moves several hops a round.
 //  * Label-correcting BFS steps (persistent engine): labels are lowered by
-//    atomicMin and a thread may label several nodes in a row over a short
-//    frontier, so one grid barrier covers several levels; reachability is
+//    atomicMin, and after expanding its share of the frontier each block
+//    expands the nodes it labelled itself for up to 16 levels from its
+//    shared-memory stage (or, as an option, a thread labels several nodes in
+//    a row), so one grid barrier covers several levels; reachability is
 //    exact in every case and labels converge to distances while lowered
 //    labels propagate.  The active queue is collected after each BFS by a
 //    streaming sweep, in node order (engine 1 appends it during its
@@ -858,12 +860,100 @@ __device__ __forceinline__ void tile_relabel(const SolveView& g, uint32_t t, uin
     __syncthreads();   // the shared tile is the next tile's
 }
 
+// One frontier node u with label hu, expanded: every neighbour v with a
+// residual arc v -> u and a label above hu + 1 (UNVIS included) is lowered
+// to hu + 1 by atomicMin and staged when that is its first label or, with
+// `propagate`, a lower one (the rule of bfs_step_body without the chain).
+__device__ __forceinline__ void bfs_expand_one(const SolveView& g, uint32_t u, uint32_t hu,
+                                               const Stage& st, bool propagate,
+                                               unsigned long long& visits)
+{
+    uint32_t arcs;
+    const int4 nb4 = residual_in_arcs(g, u, &arcs);
+    const int nb[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+    const uint32_t cand = hu + 1u;
+    ++visits;
+    uint32_t hv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) hv[k] = ((arcs >> k) & 1u) ? ldcg(g.height + nb[k]) : 0u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!((arcs >> k) & 1u) || hv[k] <= cand) continue;
+        const uint32_t old = atomicMin(g.height + nb[k], cand);
+        if (old <= cand || (old != UNVIS && !propagate)) continue;
+        stage_push(g, st, (uint32_t)nb[k]);
+    }
+}
+
+// A BFS step of the persistent engine with block sub-levels (option
+// bfs_block_levels = K > 1): each block expands its share of the frontier
+// (level L), then, without a grid barrier, the nodes it labelled itself, for
+// up to K - 1 more levels, breadth first, from its shared-memory stage (two
+// halves of stage_cap / 2 entries, ping-pong); only the last sub-level's
+// nodes, and any that overflow a half, go to the next step's queue.  Labels
+// are corrected like the chained steps' (atomicMin, re-queued while
+// `propagate`): a node labelled here before another block reaches it by a
+// shorter path is lowered and expanded again.  Frontier entries may carry
+// different labels: each expansion reads its node's label.
+__device__ __forceinline__ void bfs_step_levels_body(const SolveView& g, uint32_t L, uint32_t cnt,
+                                                     uint32_t first, uint32_t* s_fr,
+                                                     uint32_t stage_cap, uint32_t* s_m,
+                                                     unsigned long long& visits, int levels,
+                                                     bool propagate, bool exact)
+{
+    Ctl* ctl = g.ctl;
+    const uint32_t* in = (L & 1) ? g.fr[1] : g.fr[0];
+    uint32_t* out = (L & 1) ? g.fr[0] : g.fr[1];
+    uint32_t* gcnt = &ctl->bfs_cnt[(L + 1) % 3];
+    const uint32_t half = stage_cap / 2u;
+    for (uint32_t it = 0; it * (gridDim.x * DTPB) < cnt; ++it) {
+        uint32_t* cur = s_fr;
+        uint32_t* nxt = s_fr + half;
+        {
+            const Stage st{cur, &s_m[0], half, gcnt, out};
+            const uint32_t i = queue_index(it, cnt);
+            if (i < cnt) {
+                const uint32_t u = (it == 0 && cnt <= SPREAD_MAX) ? first : __ldcg(in + i);
+                bfs_expand_one(g, u, exact ? L : ldcg(g.height + u), st, propagate, visits);
+            }
+        }
+        __syncthreads();
+        for (int k = 1; k < levels; ++k) {
+            const uint32_t c = min(s_m[0], half);
+            __syncthreads();   // every thread has read the count
+            if (c == 0u) break;
+            if (threadIdx.x == 0) s_m[0] = 0u;
+            __syncthreads();
+            const Stage st{nxt, &s_m[0], half, gcnt, out};
+            for (uint32_t j = threadIdx.x; j < c; j += DTPB) {
+                const uint32_t u = cur[j];
+                bfs_expand_one(g, u, ldcg(g.height + u), st, propagate, visits);
+            }
+            __syncthreads();
+            uint32_t* tmp = cur;
+            cur = nxt;
+            nxt = tmp;
+        }
+        if (threadIdx.x == 0) {
+            s_m[2] = min(s_m[0], half);
+            s_m[0] = 0;
+            s_m[4] = s_m[2] ? atomicAdd(gcnt, s_m[2]) : 0u;
+        }
+        __syncthreads();
+        flush_stage(cur, s_m[2], s_m[4], out, g.n, ctl);
+        __syncthreads();
+    }
+}
+
 // Frontier entries block 0 keeps in shared memory in a tail step, and the
 // most levels one tail step covers (a bound on the other blocks' barrier wait).
 constexpr uint32_t TAIL_CAP = DTPB * 4u;
 constexpr int TAIL_LEVELS = 4096;
 // Default frontier size up to which tail steps run (0: none).
 constexpr uint32_t BFS_TAIL_DEFAULT = 0u;
+// Levels a block expands per BFS step from its own stage by default
+// (bfs_step_levels_body).
+constexpr int BFS_BLOCK_LEVELS = 16;
 // Free nodes from which the persistent engine relabels by tiles by default.
 constexpr uint32_t RELABEL_TILES_DEFAULT_MIN = 0xFFFFFFFFu;
 
@@ -1417,6 +1507,16 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
                     ++bu_j;
                     exact = false;
                     if (lead) ++ctl->bu_steps;
+                } else if (g.bfs_block_levels > 1) {
+                    // expansions this step: the frontier, then per block and
+                    // pass at most one stage half per sub-level
+                    const unsigned long long nn = g.n;
+                    const unsigned long long passes = (cnt + gridDim.x * DTPB - 1u) / (gridDim.x * DTPB);
+                    const unsigned long long ex_max =
+                        cnt + (unsigned long long)(g.bfs_block_levels - 1) * (DTPB * 4u) * gridDim.x * passes;
+                    bfs_step_levels_body(g, L, cnt, first, s_buf, DTPB * 8, s_m, bfs_visits,
+                                         g.bfs_block_levels, 4ull * ex_max <= nn, exact);
+                    exact = false;
                 } else {
                     const unsigned long long nn = g.n;
                     const int hops = (g.bfs_hops > 1 && cnt <= g.bfs_chain_max &&
@@ -1633,6 +1733,7 @@ SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw, 
         if (o->bfs_chain_max_frontier > 0) r.bfs_chain_max_frontier = o->bfs_chain_max_frontier;
         r.bfs_bottom_up = o->bfs_bottom_up;
         r.relabel_tiles = o->relabel_tiles;
+        r.bfs_block_levels = o->bfs_block_levels;
         if (o->bfs_bottom_up_ratio > 0) r.bfs_bottom_up_ratio = o->bfs_bottom_up_ratio;
     }
     // clamps of gpu_push_relabel_fast.cu:421-424 and :476-480
@@ -1683,16 +1784,18 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     // resident blocks per SM: a step of a small graph is one chain of
     // dependent L2 round trips plus a grid barrier whose cost grows with the
     // number of blocks, while a large graph needs the threads to cover its
-    // frontiers (measured on B200: 1 is best below ~1.5M free nodes, 4 at
-    // ~77M)
+    // frontiers and its blocks' BFS sub-levels.  Measured on B200 with the
+    // default BFS steps (15 graphs of 0.24-7.4M free nodes, three generators
+    // and the config-1 Delaunay proxy, median of 7): 2 is best or within 3%
+    // below 1.5M free nodes, 3 up to ~5M, 4 above (config 1: 3.3 ms at 2,
+    // 1.20 at 3; a 5.6M-node torus 5.07 at 3, 4.87 at 4).
     // An autotuned entry for this size class replaces the rule.
     TuneEntry te;
     const bool tuned = tune_lookup(g.n, &te);
     const int want = opt.blocks_per_sm > 0 ? opt.blocks_per_sm
                      : tuned                ? te.blocks_per_sm
-                     : g.n < 1500000u       ? 1
-                     : g.n < 6000000u       ? 2
-                     : g.n < 40000000u      ? 3
+                     : g.n < 1500000u       ? 2
+                     : g.n < 5000000u       ? 3
                                             : 4;
     int used = want < bps ? want : bps;
     if (opt.max_blocks_per_sm > 0 && used > opt.max_blocks_per_sm) used = opt.max_blocks_per_sm;
@@ -1731,6 +1834,13 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     // autotuner may pick another setting.
     gv.chain_hops = opt.chain_hops > 0 ? opt.chain_hops : tuned ? te.chain_hops : 4;
     gv.bfs_hops = opt.bfs_chain_hops > 0 ? std::min(opt.bfs_chain_hops, 64) : BFS_CHAIN_HOPS;
+    // BFS steps expand BFS_BLOCK_LEVELS levels per block by default (measured
+    // against per-thread chains of 4: benchmark graph 77.7 -> 68.0 ms, 8M-tet
+    // open box 14.1 -> 12.5 ms, 3M-tet torus 2.27 -> 1.98 ms; 8 and 32 levels
+    // within 1-3% of 16); 1 keeps the chains
+    gv.bfs_block_levels = opt.bfs_block_levels == 1 ? 0
+                          : opt.bfs_block_levels > 1 ? std::min(opt.bfs_block_levels, 64)
+                                                     : BFS_BLOCK_LEVELS;
     gv.warp_agg = agg ? 1 : 0;
     // BFS steps chain over frontiers of any size the queue bound allows
     // (measured against a 65,536-node limit: benchmark graph 78.3 -> 77.2 ms,

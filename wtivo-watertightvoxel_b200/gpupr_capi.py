@@ -66,7 +66,7 @@ class SolveOptions(ctypes.Structure):
         ("bfs_bottom_up", ctypes.c_int32), ("bfs_bottom_up_ratio", ctypes.c_double),
         ("bfs_chain_hops", ctypes.c_int32), ("bfs_tail_max", ctypes.c_int32),
         ("discharge_warp_aggregate", ctypes.c_int32), ("bfs_chain_max_frontier", ctypes.c_int32),
-        ("relabel_tiles", ctypes.c_int32),
+        ("relabel_tiles", ctypes.c_int32), ("bfs_block_levels", ctypes.c_int32),
     ]
 
 
