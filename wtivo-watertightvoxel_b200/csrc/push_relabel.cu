@@ -864,9 +864,10 @@ __device__ __forceinline__ void tile_relabel(const SolveView& g, uint32_t t, uin
 // residual arc v -> u and a label above hu + 1 (UNVIS included) is lowered
 // to hu + 1 by atomicMin and staged when that is its first label or, with
 // `propagate`, a lower one (the rule of bfs_step_body without the chain).
+// With direction-optimizing relabels, first labels are counted in s_m[6].
 __device__ __forceinline__ void bfs_expand_one(const SolveView& g, uint32_t u, uint32_t hu,
                                                const Stage& st, bool propagate,
-                                               unsigned long long& visits)
+                                               unsigned long long& visits, uint32_t* s_m)
 {
     uint32_t arcs;
     const int4 nb4 = residual_in_arcs(g, u, &arcs);
@@ -880,6 +881,7 @@ __device__ __forceinline__ void bfs_expand_one(const SolveView& g, uint32_t u, u
     for (int k = 0; k < 4; ++k) {
         if (!((arcs >> k) & 1u) || hv[k] <= cand) continue;
         const uint32_t old = atomicMin(g.height + nb[k], cand);
+        if (g.bottom_up && old == UNVIS) atomicAdd(&s_m[6], 1u);   // a first label
         if (old <= cand || (old != UNVIS && !propagate)) continue;
         stage_push(g, st, (uint32_t)nb[k]);
     }
@@ -914,7 +916,7 @@ __device__ __forceinline__ void bfs_step_levels_body(const SolveView& g, uint32_
             const uint32_t i = queue_index(it, cnt);
             if (i < cnt) {
                 const uint32_t u = (it == 0 && cnt <= SPREAD_MAX) ? first : __ldcg(in + i);
-                bfs_expand_one(g, u, exact ? L : ldcg(g.height + u), st, propagate, visits);
+                bfs_expand_one(g, u, exact ? L : ldcg(g.height + u), st, propagate, visits, s_m);
             }
         }
         __syncthreads();
@@ -927,7 +929,7 @@ __device__ __forceinline__ void bfs_step_levels_body(const SolveView& g, uint32_
             const Stage st{nxt, &s_m[0], half, gcnt, out};
             for (uint32_t j = threadIdx.x; j < c; j += DTPB) {
                 const uint32_t u = cur[j];
-                bfs_expand_one(g, u, ldcg(g.height + u), st, propagate, visits);
+                bfs_expand_one(g, u, ldcg(g.height + u), st, propagate, visits, s_m);
             }
             __syncthreads();
             uint32_t* tmp = cur;
@@ -938,6 +940,10 @@ __device__ __forceinline__ void bfs_step_levels_body(const SolveView& g, uint32_
             s_m[2] = min(s_m[0], half);
             s_m[0] = 0;
             s_m[4] = s_m[2] ? atomicAdd(gcnt, s_m[2]) : 0u;
+            if (g.bottom_up && s_m[6]) {
+                atomicAdd(&ctl->lab_cnt[(L + 1) % 3], s_m[6]);
+                s_m[6] = 0;
+            }
         }
         __syncthreads();
         flush_stage(cur, s_m[2], s_m[4], out, g.n, ctl);
