@@ -69,11 +69,11 @@ WORKLOAD = "torus-knot (3,5) tube, 2% patches dropped, inner shell 0.002, noise 
 # reads nbr 16 + res 16 + rev 1 + term 4 + excess 8 + height 4 + 4 neighbour
 # heights 16, queue read+write 8 = 73 B; each push adds res+reverse res 8 and
 # two excess updates 16 = 24 B; a BFS frontier expansion reads the node's
-# in-arc row 16 + 4 neighbour heights 16 and writes a label + queue entry 8 =
-# 40 B; every global relabel streams over each node twice: the seed (term 4,
-# height write 4, nbr 16 + pair 16 + res 16 read and the in-arc row 16
-# written) and the active sweep (height 4 + excess 8) = 84 B.
-B_VISIT, B_PUSH, B_BFS, B_SWEEP = 73, 24, 40, 84
+# neighbour row 16 and in-arc mask 1 + 4 neighbour heights 16 and writes a
+# label + queue entry 8 = 41 B; every global relabel streams over each node
+# twice: the seed (term 4, height write 4, pair 16 + res 16 read and the
+# in-arc mask 1 written) and the active sweep (height 4 + excess 8) = 53 B.
+B_VISIT, B_PUSH, B_BFS, B_SWEEP = 73, 24, 41, 53
 
 
 LEGS = ("e2e", "cpu", "batch", "serve", "labels", "audit", "raw", "config1", "noalloc", "autotune",

@@ -20,13 +20,15 @@
 extern "C" {
 #endif
 
-#define GPUPR_ABI_VERSION 4   /* 2: stats and options carry the persistent engine's
+#define GPUPR_ABI_VERSION 5   /* 2: stats and options carry the persistent engine's
                                  grid, relabel factor and chaining; tuning entries.
                                  3: stats carry the active-sweep time, the graphs
                                  a batch retired early and the bottom-up steps;
                                  options carry the direction-optimizing BFS switch.
                                  4: options carry relabel_tiles, stats the tile
-                                 steps (53 eight-byte stats fields) */
+                                 steps (53 eight-byte stats fields).
+                                 5: options carry bfs_block_levels and
+                                 bfs_in_arc_masks */
 
 typedef enum {
     GPUPR_OK = 0,
@@ -170,6 +172,13 @@ typedef struct {
                                      (breadth first, shared-memory stage);
                                      0 = default (16), 1 = per-thread chains
                                      instead (bfs_chain_hops, bfs_chain_max_frontier) */
+    int32_t bfs_in_arc_masks;     /* persistent engine, frontier steps: 1 = each
+                                     relabel's seed sweep writes one byte per node
+                                     (which neighbours have a residual arc into
+                                     it) and a BFS step reads the node's
+                                     neighbour row with it; < 0 = the sweep writes
+                                     a 16-byte in-arc row per node instead;
+                                     0 = default */
 } gpupr_solve_options;
 
 const char* gpupr_status_string(gpupr_status status);

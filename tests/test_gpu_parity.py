@@ -115,7 +115,10 @@ def test_solver_invariants(built, kind, seed, size):
                                  dict(relabel_tiles=1, bfs_bottom_up=1, bfs_tail_max=1024),
                                  dict(relabel_tiles=1, engine=1),
                                  dict(bfs_block_levels=1), dict(bfs_block_levels=4), dict(bfs_block_levels=2, blocks_per_sm=1),
-                                 dict(bfs_block_levels=16, work_relabel_factor=0.05)])
+                                 dict(bfs_block_levels=16, work_relabel_factor=0.05),
+                                 dict(bfs_in_arc_masks=1), dict(bfs_in_arc_masks=-1),
+                                 dict(bfs_in_arc_masks=1, bfs_block_levels=1),
+                                 dict(bfs_in_arc_masks=1, bfs_bottom_up=1, bfs_bottom_up_ratio=1e9)])
 def test_options_do_not_change_the_cut(built, opt):
     import gpupr_capi
 

@@ -96,6 +96,9 @@ struct SolveView {
                                         // with a residual arc into it (-1 elsewhere),
                                         // written by each relabel's seed sweep (null:
                                         // the BFS derives them from pair and res)
+    uint8_t* inm;                       // [n] persistent engine, instead of inrow: bit k
+                                        // = residual arc nbr[v][k] -> v, written by each
+                                        // relabel's seed sweep from pair and res
     int32_t* term;                      // [n] src - snk residual
     long long* excess;                  // [n]
     uint32_t* height;                   // [n]
@@ -307,6 +310,8 @@ struct SolveOptions {
     int relabel_tiles = 0;         // persistent engine: 1 = tiled relabels, < 0 = frontier
                                    // steps, 0 = default
     int bfs_block_levels = 0;      // persistent engine: > 1 = block sub-levels per BFS step
+    int bfs_in_arc_masks = 0;      // persistent engine: 1 = in-arc masks, < 0 = in-arc rows,
+                                   // 0 = default
 };
 
 SolveOptions resolve_options(const gpupr_solve_options* o, int local_steps_raw,
@@ -320,13 +325,14 @@ struct SolveWorkspace {
     DevBuf<uint32_t> chunk_seg, seg_live, seg_act;   // segmented solves only
     DevBuf<uint32_t> cand0, cand1;                   // direction-optimizing relabels only
     DevBuf<int4> inrow;                              // persistent engine: in-arc rows
+    DevBuf<uint8_t> inm;                             // persistent engine: in-arc masks
     DevBuf<uint8_t> arcm;                            // tiled relabels: arc masks
     DevBuf<uint32_t> tile_stamp;                     // tiled relabels: queue stamps
     uint64_t bytes() const
     {
         return excess.bytes() + height.bytes() + q0.bytes() + q1.bytes() + q2.bytes() + ctl.bytes() +
                chunk_seg.bytes() + seg_live.bytes() + seg_act.bytes() + cand0.bytes() + cand1.bytes() +
-               inrow.bytes() + arcm.bytes() + tile_stamp.bytes();
+               inrow.bytes() + inm.bytes() + arcm.bytes() + tile_stamp.bytes();
     }
 };
 

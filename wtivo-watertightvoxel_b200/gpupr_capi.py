@@ -67,6 +67,7 @@ class SolveOptions(ctypes.Structure):
         ("bfs_chain_hops", ctypes.c_int32), ("bfs_tail_max", ctypes.c_int32),
         ("discharge_warp_aggregate", ctypes.c_int32), ("bfs_chain_max_frontier", ctypes.c_int32),
         ("relabel_tiles", ctypes.c_int32), ("bfs_block_levels", ctypes.c_int32),
+        ("bfs_in_arc_masks", ctypes.c_int32),
     ]
 
 
