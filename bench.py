@@ -382,7 +382,12 @@ def run_ours(args, world, rank, local):
                 "bfs_steps_by_frontier": {"le_1024": int(stats[-1]["bfs_steps_by_frontier"][0]),
                                           "le_16384": int(stats[-1]["bfs_steps_by_frontier"][1]),
                                           "larger": int(stats[-1]["bfs_steps_by_frontier"][2]),
-                                          "ms": [round(x, 3) for x in stats[-1]["bfs_ms_by_frontier"]]}}
+                                          "ms": [round(x, 3) for x in stats[-1]["bfs_ms_by_frontier"]]},
+                "discharge_rounds_by_active": {
+                    "le_4096": int(stats[-1]["discharge_rounds_by_active"][0]),
+                    "le_131072": int(stats[-1]["discharge_rounds_by_active"][1]),
+                    "larger": int(stats[-1]["discharge_rounds_by_active"][2]),
+                    "ms": [round(x, 3) for x in stats[-1]["discharge_ms_by_active"]]}}
     if rank == 0:
         rs = random_sector_rate(dev)
         roofline["random_sector_gbs"] = round(rs, 1)

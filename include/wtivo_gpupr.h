@@ -20,7 +20,7 @@
 extern "C" {
 #endif
 
-#define GPUPR_ABI_VERSION 5   /* 2: stats and options carry the persistent engine's
+#define GPUPR_ABI_VERSION 6   /* 2: stats and options carry the persistent engine's
                                  grid, relabel factor and chaining; tuning entries.
                                  3: stats carry the active-sweep time, the graphs
                                  a batch retired early and the bottom-up steps;
@@ -28,7 +28,10 @@ extern "C" {
                                  4: options carry relabel_tiles, stats the tile
                                  steps (53 eight-byte stats fields).
                                  5: options carry bfs_block_levels and
-                                 bfs_in_arc_masks */
+                                 bfs_in_arc_masks.
+                                 6: stats carry the discharge rounds and their
+                                 time by active-set size (59 eight-byte stats
+                                 fields) */
 
 typedef enum {
     GPUPR_OK = 0,
@@ -103,6 +106,10 @@ typedef struct {
     uint64_t tile_procs;        /* ... tiles processed */
     uint64_t tile_loads;        /* ... nodes those tiles loaded */
     uint64_t tile_writes;       /* ... labels lowered */
+    uint64_t discharge_rounds_by_active[3]; /* persistent engine: discharge rounds
+                                           over <= 4096, <= 131072 and more
+                                           active nodes */
+    double discharge_ms_by_active[3];       /* ... and their time (block 0's clock) */
 } gpupr_cut_stats;
 
 /* Solver tuning knobs; zero fields take the defaults shown. */

@@ -19,7 +19,7 @@ def test_library_exports_header(built):
     L = ctypes.CDLL(str(gpupr_capi.LIB_PATH))
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
-    assert gpupr_capi.lib().gpupr_abi_version() == 5
+    assert gpupr_capi.lib().gpupr_abi_version() == 6
     assert gpupr_capi.lib().gpupr_status_string(9) == b"GPUPr-FAST-v6.30 max macro rounds exceeded"
 
 

@@ -222,6 +222,10 @@ void run_graph_cut(const double* vertices, uint64_t nv, int v_dev, const int32_t
         st->bfs_steps_by_frontier[k] = sr.step_cnt[k];
         st->bfs_ms_by_frontier[k] = sr.step_ms[k];
     }
+    for (int k = 0; k < 3; ++k) {
+        st->discharge_rounds_by_active[k] = sr.dround_cnt[k];
+        st->discharge_ms_by_active[k] = sr.dround_ms[k];
+    }
     st->bfs_tail_steps = sr.tail_steps;
     st->bfs_tail_levels = sr.tail_levels;
     st->relabel_tiles = sr.relabel_tiles;
@@ -554,6 +558,10 @@ void run_graph_cut_batch(uint32_t G, const uint64_t* toff, const uint64_t* voff,
         st->bfs_steps_by_frontier[k] = sr.step_cnt[k];
         st->bfs_ms_by_frontier[k] = sr.step_ms[k];
     }
+    for (int k = 0; k < 3; ++k) {
+        st->discharge_rounds_by_active[k] = sr.dround_cnt[k];
+        st->discharge_ms_by_active[k] = sr.dround_ms[k];
+    }
     st->bfs_tail_steps = sr.tail_steps;
     st->bfs_tail_levels = sr.tail_levels;
     st->relabel_tiles = sr.relabel_tiles;
@@ -808,6 +816,10 @@ gpupr_status gpupr_solve_reduced(uint32_t n, int32_t* d_neighbors, uint32_t* d_r
                 stats->bfs_steps_by_frontier[k] = sr.step_cnt[k];
                 stats->bfs_ms_by_frontier[k] = sr.step_ms[k];
             }
+            for (int k = 0; k < 3; ++k) {
+                stats->discharge_rounds_by_active[k] = sr.dround_cnt[k];
+                stats->discharge_ms_by_active[k] = sr.dround_ms[k];
+            }
             stats->bfs_tail_steps = sr.tail_steps;
             stats->bfs_tail_levels = sr.tail_levels;
             stats->relabel_tiles = sr.relabel_tiles;
@@ -883,6 +895,10 @@ gpupr_status gpupr_solve_ell(uint32_t n, const int32_t* d_nbr, const uint32_t* d
             for (int k = 0; k < 3; ++k) {
                 stats->bfs_steps_by_frontier[k] = sr.step_cnt[k];
                 stats->bfs_ms_by_frontier[k] = sr.step_ms[k];
+            }
+            for (int k = 0; k < 3; ++k) {
+                stats->discharge_rounds_by_active[k] = sr.dround_cnt[k];
+                stats->discharge_ms_by_active[k] = sr.dround_ms[k];
             }
             stats->bfs_tail_steps = sr.tail_steps;
             stats->bfs_tail_levels = sr.tail_levels;

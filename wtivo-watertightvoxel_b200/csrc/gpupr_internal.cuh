@@ -67,6 +67,10 @@ struct Ctl {
     unsigned long long tile_procs;
     unsigned long long tile_loads;
     unsigned long long tile_writes;
+    // persistent engine: discharge rounds by active-set size (<= 4096,
+    // <= 131072, larger) and block 0's time in each class
+    uint32_t dround_cnt[3];
+    unsigned long long dround_ns[3];
 };
 
 // Nodes per tile of a tiled relabel (a power of two; the persistent engine
@@ -362,6 +366,8 @@ struct SolveResult {
     int chain_hops = 0, chain_max_active = 0;   // persistent engine: chaining used
     int relabel_tiles = 0;         // persistent engine: 1 = tiled relabels ran
     uint64_t tile_steps = 0, tile_procs = 0, tile_loads = 0, tile_writes = 0;
+    uint64_t dround_cnt[3] = {0, 0, 0};  // discharge rounds by active nodes (<= 4096, <= 131072, larger)
+    double dround_ms[3] = {0, 0, 0};
 };
 
 // Autotuner table (push_relabel.cu): per size class (floor(log2 n)), the

@@ -1450,6 +1450,8 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
     __shared__ unsigned long long s_clk[4];
     __shared__ unsigned long long s_step_ns[3];
     __shared__ uint32_t s_step_cnt[3];
+    __shared__ unsigned long long s_dr_ns[3], s_dr_t0;
+    __shared__ uint32_t s_dr_cnt[3];
     auto lap = [&](int phase) {
         if (lead) {
             const unsigned long long t = gtimer();
@@ -1478,7 +1480,7 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
         if (lead) {
             s_clk[0] = s_clk[1] = s_clk[2] = 0ull;
             s_clk[3] = gtimer();
-            for (int k = 0; k < 3; ++k) { s_step_ns[k] = 0ull; s_step_cnt[k] = 0u; }
+            for (int k = 0; k < 3; ++k) { s_step_ns[k] = 0ull; s_step_cnt[k] = 0u; s_dr_ns[k] = 0ull; s_dr_cnt[k] = 0u; }
         }
         while (ok) {
             // ---- global relabel (label-correcting steps, reachability exact) ----
@@ -1606,8 +1608,14 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
                     break;
                 }
                 if (lead) ctl->act_cnt[(r + 2) % 3] = 0u;
+                if (lead) s_dr_t0 = gtimer();   // shared: keeps the discharge's registers free
                 discharge_body<kAgg>(g, r, cnt, first, s_buf, DTPB * 8, s_m, w);
                 if (!(ok = grid_barrier(ctl, bar_target, deadline, p.wait_ns, &s_ok))) break;
+                if (lead) {
+                    const int c = cnt <= 4096u ? 0 : (cnt <= 131072u ? 1 : 2);
+                    s_dr_ns[c] += gtimer() - s_dr_t0;
+                    ++s_dr_cnt[c];
+                }
                 ++r;
                 ++rounds_total;
                 visits += cnt;
@@ -1644,6 +1652,8 @@ __global__ void __launch_bounds__(DTPB, 4) k_solve_persistent(SolveView g, Persi
             for (int k = 0; k < 3; ++k) {
                 ctl->step_cnt[k] = s_step_cnt[k];
                 ctl->step_ns[k] = s_step_ns[k];
+                ctl->dround_cnt[k] = s_dr_cnt[k];
+                ctl->dround_ns[k] = s_dr_ns[k];
             }
             ctl->bfs_ns = s_clk[0];
             ctl->sweep_ns = s_clk[1];
@@ -1945,6 +1955,8 @@ void solve_persistent(const SolveView& g, const SolveOptions& opt, cudaStream_t 
     for (int k = 0; k < 3; ++k) {
         out.step_cnt[k] = hc.step_cnt[k];
         out.step_ms[k] = (double)hc.step_ns[k] * 1e-6;
+        out.dround_cnt[k] = hc.dround_cnt[k];
+        out.dround_ms[k] = (double)hc.dround_ns[k] * 1e-6;
     }
     out.solve_s = std::chrono::duration<double>(Clock::now() - t0).count();
 }

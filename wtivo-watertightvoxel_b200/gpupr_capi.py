@@ -44,6 +44,8 @@ STATS_FIELDS = [
     ("relabel_tiles", ctypes.c_int64), ("tile_steps", ctypes.c_uint64),
     ("tile_procs", ctypes.c_uint64), ("tile_loads", ctypes.c_uint64),
     ("tile_writes", ctypes.c_uint64),
+    ("discharge_rounds_by_active", ctypes.c_uint64 * 3),
+    ("discharge_ms_by_active", ctypes.c_double * 3),
 ]
 
 
