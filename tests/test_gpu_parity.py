@@ -131,6 +131,27 @@ def test_options_do_not_change_the_cut(built, opt):
     assert st["adjusted_flow"] == st0["adjusted_flow"]
 
 
+def test_step_histograms_add_up(built):
+    """The persistent engine's per-class counters cover every discharge round
+    and BFS step of a solve, and their times fit inside the solve; with the
+    bottom-up switch forced on, the default (block sub-level) BFS steps hand
+    over to bottom-up steps, and the cut stays the same."""
+    import gpupr_capi
+
+    g = cached_graph("lattice", 3, 300_000)
+    tets, nbrs = to_cuda(g["tets"], g["neighbors"])
+    base, st = gpupr_capi.graph_cut(g["vertices"], tets, nbrs, g["labels"], g["fill_T"])
+    assert int(st["engine"]) == 2
+    assert sum(st["discharge_rounds_by_active"]) == int(st["rounds"])
+    assert sum(st["bfs_steps_by_frontier"]) + int(st["bottom_up_steps"]) >= 1
+    assert 0.0 < sum(st["discharge_ms_by_active"]) <= st["solve_device_ms"]
+    assert sum(st["bfs_ms_by_frontier"]) <= st["solve_device_ms"]
+    out, st2 = gpupr_capi.graph_cut(g["vertices"], tets, nbrs, g["labels"], g["fill_T"],
+                                    opts=gpupr_capi.options(bfs_bottom_up=1, bfs_bottom_up_ratio=64.0))
+    assert int(st2["bottom_up_steps"]) > 0
+    assert np.array_equal(out, base) and st2["adjusted_flow"] == st["adjusted_flow"]
+
+
 def test_device_resident_inputs(built):
     import gpupr_capi
 
