@@ -149,25 +149,50 @@ struct Staging {
     bool ok = false;
 };
 
-// Staging of one device and direction (0 = to device, 1 = to host), made on
-// first use with that device current.
-Staging& staging(int dir)
+// Staging sets per device and direction (0 = to device, 1 = to host) that
+// host threads can hold at the same time, so that copies issued by
+// different threads (the server's two lanes, each uploading its own batch)
+// run side by side instead of queueing on one set; each set is kSlots x
+// kChunk pinned bytes, made on first use with its device current.
+constexpr int kSets = 3;
+
+// A staging set held by one copy until the lease goes out of scope.
+struct StagingLease {
+    Staging* st;
+    std::unique_lock<std::mutex> lk;
+};
+
+// Takes a staging set of the current device for direction dir that no other
+// copy holds; makes one while there are fewer than kSets, else waits for the
+// first set.
+StagingLease staging(int dir)
 {
     static std::mutex mu;
-    static std::map<std::pair<int, int>, std::unique_ptr<Staging>> all;
+    static std::map<std::pair<int, int>, std::vector<std::unique_ptr<Staging>>> all;
     int dev = 0;
     GPUPR_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mu);
-    auto& st = all[{dev, dir}];
-    if (!st) {
-        auto s = std::make_unique<Staging>();
-        GPUPR_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&s->pin), kChunk * kSlots, cudaHostAllocPortable));
-        for (int i = 0; i < kSlots; ++i)
-            GPUPR_CUDA(cudaEventCreateWithFlags(&s->ev[i], cudaEventDisableTiming));
-        s->ok = true;
-        st = std::move(s);
+    Staging* first = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto& sets = all[{dev, dir}];
+        for (auto& s : sets) {
+            std::unique_lock<std::mutex> l(s->mu, std::try_to_lock);
+            if (l.owns_lock()) return {s.get(), std::move(l)};
+        }
+        if ((int)sets.size() < kSets) {
+            auto s = std::make_unique<Staging>();
+            GPUPR_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&s->pin), kChunk * kSlots, cudaHostAllocPortable));
+            for (int i = 0; i < kSlots; ++i)
+                GPUPR_CUDA(cudaEventCreateWithFlags(&s->ev[i], cudaEventDisableTiming));
+            s->ok = true;
+            std::unique_lock<std::mutex> l(s->mu);
+            Staging* p = s.get();
+            sets.push_back(std::move(s));
+            return {p, std::move(l)};
+        }
+        first = sets.front().get();
     }
-    return *st;
+    return {first, std::unique_lock<std::mutex>(first->mu)};
 }
 
 // Waits for the copies a previous call left in flight (after an error, or
@@ -200,8 +225,8 @@ void host_to_device(void* d_dst, const void* h_src, size_t bytes, cudaStream_t s
         GPUPR_CUDA(cudaMemcpyAsync(d_dst, h_src, bytes, cudaMemcpyHostToDevice, s));
         return;
     }
-    Staging& st = staging(0);
-    std::lock_guard<std::mutex> lk(st.mu);
+    StagingLease lease = staging(0);
+    Staging& st = *lease.st;
     settle(st);
     const char* src = static_cast<const char*>(h_src);
     char* dst = static_cast<char*>(d_dst);
@@ -226,8 +251,8 @@ void device_to_host(void* h_dst, const void* d_src, size_t bytes, cudaStream_t s
         GPUPR_CUDA(cudaStreamSynchronize(s));
         return;
     }
-    Staging& st = staging(1);
-    std::lock_guard<std::mutex> lk(st.mu);
+    StagingLease lease = staging(1);
+    Staging& st = *lease.st;
     settle(st);
     const char* src = static_cast<const char*>(d_src);
     char* dst = static_cast<char*>(h_dst);
@@ -265,8 +290,8 @@ void upload_topology(int32_t* d_out, const void* host, uint64_t rows, int64_t ro
         return;
     }
     const char* base = static_cast<const char*>(host);
-    Staging& st = staging(0);
-    std::lock_guard<std::mutex> lk(st.mu);
+    StagingLease lease = staging(0);
+    Staging& st = *lease.st;
     settle(st);
     const uint64_t per_chunk = kChunk / 16u;
     const uint64_t nch = (rows + per_chunk - 1) / per_chunk;

@@ -21,7 +21,10 @@
 //
 // So uploads overlap solves, requests that arrive while a batch runs join the
 // next one, and a small request never waits for a large one's solve: the two
-// lanes' solves run at the same time.  Their persistent grids are capped so
+// lanes' solves run at the same time.  A small request that arrives while the
+// small lane has work in flight and the large lane has none takes the large
+// lane (three times the small lane's grid), so a backlog of small requests
+// does not pile up on one resident block per SM while most of the GPU idles.  Their persistent grids are capped so
 // that both fit on the GPU together (small lane 1 resident block per SM, large
 // lane the kernel's occupancy limit minus one): every block of both grids can
 // be resident at once, whichever launches first, so neither grid's barrier
@@ -80,6 +83,7 @@ struct gpupr_server {
         cudaEvent_t uploaded = nullptr;
         std::deque<std::shared_ptr<Request>> pending;
         std::unique_ptr<Batch> staged;  // uploaded, waiting for the lane's solver
+        uint64_t busy_tets = 0;         // tets of the lane's requests submitted and not done
         bool stager_done = false;
         std::thread stager, solver;
     };
@@ -237,6 +241,7 @@ void gpupr_server::publish(Batch& b, const std::vector<gpupr_batch_item>* items,
         r.result.solve_ms = ms(b.t_solve, t_done);
         r.result.latency_ms = ms(r.t_submit, t_done);
         r.result.lane = r.lane;
+        if (!r.done) lanes[(size_t)r.lane]->busy_tets -= r.n;
         r.done = true;
     }
     cv.notify_all();
@@ -430,6 +435,11 @@ gpupr_status gpupr_server_submit(gpupr_server* sv, const double* vertices, uint6
             gpupr::set_last_error("the server is shutting down");
             return GPUPR_ERR_INVALID_ARGUMENT;
         }
+        // a small request spills to an idle large lane while the small lane is busy
+        if (r->lane == 0 && sv->lanes.size() == 2 && sv->lanes[0]->busy_tets > 0 &&
+            sv->lanes[1]->busy_tets == 0)
+            r->lane = 1;
+        sv->lanes[(size_t)r->lane]->busy_tets += r->n;
         r->id = sv->next_id++;
         sv->all[r->id] = r;
         sv->lanes[(size_t)r->lane]->pending.push_back(r);
