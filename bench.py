@@ -1064,7 +1064,8 @@ def run_serve(args):
     seeded graphs), 160 GiB admission budget, host arrays in and out.  At 20
     req/s (the config's rate) and at 100 req/s (a load where requests queue),
     the same arrival trace goes through the server with its two lanes (small
-    requests below 2M tets solve beside large ones), through one lane
+    requests below 2M tets solve beside large ones, or on the large lane while
+    it is idle and the small lane busy), through one lane
     (continuous batching, one solve at a time), and through one lane one
     request at a time (max_batch 1); the 20 req/s trace is also replayed
     against one-at-a-time service times measured alone (the naive FIFO).
