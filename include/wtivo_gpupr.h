@@ -302,7 +302,9 @@ typedef struct {
  * (its persistent grid capped at 1 resident block per SM), the rest to the
  * large lane (capped at the solver kernel's occupancy limit minus one), so
  * both lanes' grids are resident together and a small request never waits
- * for a large one's solve.  The HBM budget covers both lanes.
+ * for a large one's solve.  A small request submitted while the small lane
+ * has work in flight and the large lane has none takes the large lane
+ * (gpupr_request_result.lane says which).  The HBM budget covers both lanes.
  * gpupr_server_create_lanes takes the split; split_tets = 0 gives one lane
  * (every solve on the whole GPU, one at a time). */
 gpupr_status gpupr_server_create(uint64_t hbm_budget_bytes, uint32_t max_batch,
