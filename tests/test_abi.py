@@ -168,6 +168,27 @@ def test_python_structs_match_the_header(tmp_path):
             assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, (cname, f)
 
 
+def test_integration_stub_matches_the_stats_struct():
+    """The ctypes stub a maintainer would paste from INTEGRATION.md declares
+    as many eight-byte fields as gpupr_cut_stats has, and names the ABI
+    version the library reports."""
+    import re
+    from pathlib import Path
+
+    import gpupr_capi
+
+    text = (Path(__file__).resolve().parents[1] / "INTEGRATION.md").read_text()
+    m = re.search(r"class Stats\(ctypes.Structure\):.*?\((\d+) eight-byte fields, ABI (\d+)\).*?"
+                  r"_fields_ = \[(.*?)\] \+ \\\s*\[\(\"pad%d\" % i, ctypes.c_uint64\) for i in range\((\d+)\)\]",
+                  text, flags=re.S)
+    assert m, "Stats stub not found in INTEGRATION.md"
+    fields, abi, named, pads = int(m.group(1)), int(m.group(2)), m.group(3), int(m.group(4))
+    n_named = named.count("ctypes.c_")
+    assert ctypes.sizeof(gpupr_capi.CutStats) == 8 * fields == 8 * (n_named + pads)
+    header = gpupr_capi.HEADER.read_text()
+    assert int(re.search(r"#define GPUPR_ABI_VERSION (\d+)", header).group(1)) == abi
+
+
 def test_every_header_function_has_argtypes(built):
     """The ctypes binding declares argument types for every function the
     header declares (an undeclared one would be called with guessed types)."""
